@@ -1,0 +1,178 @@
+/*
+ * mgagcd.h -- C ABI of the B200 Louvain engine (libmgagcd.so).
+ *
+ * The reference (MG-alphaGCD) has no plugin or FFI layer: its boundary is the
+ * in-process C++ call chain driven by the MG_GCD binary (src/main.cu:118-131).
+ * Each entry point below names the reference interface it replaces.  All
+ * entry points return mg_status (never exit, never throw across the ABI);
+ * mg_last_error() gives the text of the last failure on a context.
+ *
+ * Ownership: the library owns every mg_graph / mg_result it returns; the
+ * caller releases them with the matching *_destroy.  Host buffers passed in
+ * are only read during the call; output buffers are sized by the caller as
+ * documented.  A context is bound to one CUDA device and one host thread at a
+ * time.
+ */
+#ifndef MGAGCD_H
+#define MGAGCD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    MG_OK = 0,
+    MG_ERR_INVALID = 1,     /* bad argument / handle */
+    MG_ERR_CUDA = 2,        /* CUDA runtime error */
+    MG_ERR_OOM = 3,         /* device or host allocation failed / over budget */
+    MG_ERR_IO = 4,          /* file cannot be opened */
+    MG_ERR_FORMAT = 5,      /* malformed .mtx input */
+    MG_ERR_UNSUPPORTED = 6, /* size or mode outside what the engine supports */
+    MG_ERR_TIMEOUT = 7,     /* a bounded device wait or probe gave up */
+    MG_ERR_CANCELLED = 8    /* job cancelled */
+} mg_status;
+
+typedef struct mg_ctx mg_ctx;
+typedef struct mg_graph mg_graph;
+typedef struct mg_result mg_result;
+
+/* weight element types for mg_graph_from_csr */
+enum { MG_WEIGHT_UNIT = 0, MG_WEIGHT_F32 = 1, MG_WEIGHT_F64 = 2 };
+
+/* precision modes of the local-move gain (mg_run_opts.precision) */
+enum {
+    MG_PREC_FP64 = 0,  /* the reference's double arithmetic (default) */
+    MG_PREC_INT64 = 1, /* exact integer gain comparison; integral weights only */
+    MG_PREC_FP32 = 2   /* single-precision gains, double sigma_tot and modularity */
+};
+
+typedef struct {
+    int device;              /* CUDA device ordinal (default 0) */
+    int verbose;             /* print the reference's tables to stdout */
+    size_t hbm_budget_bytes; /* 0 = no limit */
+} mg_opts;
+
+const char *mg_status_string(mg_status s);
+const char *mg_version(void);
+
+/* Context.  Replaces the process setup of src/main.cu:28-59 (device select);
+ * no MPI / NVSHMEM init is needed on one GPU. */
+mg_status mg_init(mg_ctx **ctx, const mg_opts *opts /* may be NULL */);
+mg_status mg_destroy(mg_ctx *ctx);
+const char *mg_last_error(const mg_ctx *ctx);
+
+/* ---- graphs -------------------------------------------------------------- */
+
+/* Copy a symmetric CSR from host memory into library-owned device memory.
+ * offsets[n+1] (uint64), cols[nnz] (uint32), weights per weight_type (NULL
+ * with MG_WEIGHT_UNIT).  nnz = offsets[n] must be < 2^32.
+ * Replaces HostGraph + GpuGraph + edge_partition::partitioner for one GPU
+ * (src/graph/host_graph.cpp:3, src/graph/gpu_graph.cu:3,
+ *  src/partition/edge_partition.cu:26). */
+mg_status mg_graph_from_csr(mg_ctx *ctx, uint32_t n, const uint64_t *offsets, const uint32_t *cols,
+                            const void *weights, int weight_type, mg_graph **out);
+
+/* Same, with the arrays already in device memory (copied device-to-device). */
+mg_status mg_graph_from_device_csr(mg_ctx *ctx, uint32_t n, uint64_t nnz, const uint32_t *d_offsets32,
+                                   const uint32_t *d_cols, const void *d_weights, int weight_type,
+                                   mg_graph **out);
+
+/* Load a Matrix Market file with the reference's rules.
+ * Replaces loadMMSparseMatrix / init_data_from_mtx (src/mmio/mmio_wrapper.cu:76-301). */
+mg_status mg_graph_from_mtx(mg_ctx *ctx, const char *path, mg_graph **out);
+
+/* Seeded synthetic graphs generated on the device (integer-only RNG; the
+ * same seed gives the same graph as the CPU generators of the test oracle).
+ * Replaces HostGraph::randomly_generate_graph (src/graph/host_graph.cpp:38-77). */
+mg_status mg_graph_generate_rmat(mg_ctx *ctx, int scale, int edge_factor, double a, double b, double c,
+                                 uint64_t seed, mg_graph **out);
+mg_status mg_graph_generate_sbm(mg_ctx *ctx, uint32_t n, uint32_t blocks, double mean_degree,
+                                double intra_frac, uint64_t seed, mg_graph **out);
+
+/* n, nnz, mass (sum of all directed weights, src/graph/host_graph.cpp:112-115),
+ * integral (1 when every weight is a non-negative integer and mass < 2^32). */
+mg_status mg_graph_info(const mg_graph *g, uint32_t *n, uint64_t *nnz, double *mass, int *integral);
+/* Copy the CSR back to host buffers (offsets[n+1], cols[nnz], weights[nnz]
+ * as double; any pointer may be NULL). */
+mg_status mg_graph_copy_csr(const mg_graph *g, uint64_t *offsets, uint32_t *cols, double *weights);
+mg_status mg_graph_destroy(mg_graph *g);
+
+/* ---- stage hooks (the reference's stage boundaries) ----------------------- */
+
+/* Degree binning of the graph's rows.  scheme 0: 10 local-move bins
+ * (src/bin/BIN.cu:468-499), 1: 11 coarsen-symbolic bins (:501-540),
+ * 2: 9 coarsen-numeric bins (:542-575).  sizes/offsets: 11 slots (unused
+ * slots zero); perm[n]: items bin by bin, ascending id inside a bin. */
+mg_status mg_bins(mg_graph *g, int scheme, uint32_t *sizes, uint32_t *offsets, uint32_t *perm,
+                  uint32_t *max_degree);
+/* Same over an arbitrary offsets array (degree of item i = offsets[i+1]-offsets[i]),
+ * as BIN::bin_create(com_degree, ...) is used on community degrees. */
+mg_status mg_bins_offsets(mg_ctx *ctx, int scheme, uint32_t n, const uint64_t *offsets, uint32_t *sizes,
+                          uint32_t *bin_offsets, uint32_t *perm, uint32_t *max_degree);
+
+/* One local-move sweep from assignment C with community weights sigma and
+ * vertex weights k (host buffers of n), writing C_new.  version 2 (default
+ * reference behaviour) or 1; up = 1 for an "up" iteration.
+ * Replaces louvain::calculate_eicj_and_move_vertex_bin (src/louvain/louvain.cu:1032-1296,
+ * src/louvain/louvain_gl.cu:1018).  distinct (optional) receives the number of
+ * distinct (vertex, neighbour community) candidate pairs. */
+mg_status mg_local_move(mg_graph *g, int version, int up, int precision, const uint32_t *C,
+                        const double *sigma, const double *k, uint32_t *C_new, uint64_t *distinct);
+
+/* Modularity of an assignment (src/louvain/louvain.cu:105-238), sigma_tot
+ * computed from C. */
+mg_status mg_modularity(mg_graph *g, const uint32_t *C, double *q);
+
+/* Coarsen by assignment C: dense order-preserving relabel (written to
+ * C_dense[n] if not NULL) and the next-level graph with rows sorted by
+ * neighbour community, self-loops kept.
+ * Replaces coarsen_graph_mg::coarsen_graph (src/coarsen_graph/coarsen_graph_mg.cu:2054-2240). */
+mg_status mg_coarsen(mg_graph *g, const uint32_t *C, uint32_t *C_dense, mg_graph **out);
+
+/* ---- full Louvain ----------------------------------------------------------- */
+
+typedef struct {
+    int version;       /* 0, 1 or 2 (src/main.cu:118-131); 0 behaves as 2 on one GPU */
+    double threshold;  /* default 1e-6 (src/main.cu:21) */
+    int max_phases;    /* default 1000 (src/main.cu:23) */
+    int precision;     /* MG_PREC_* */
+    int verbose;       /* print the reference's per-phase tables */
+} mg_run_opts;
+
+typedef struct {
+    double modularity;       /* final Q */
+    int phases;              /* coarsening steps taken */
+    int levels;              /* phases started */
+    int iterations;          /* local-move sweeps */
+    uint32_t communities;    /* final community count */
+    double seconds_total;    /* device time of the whole run */
+    double seconds_local_move;
+    double seconds_coarsen;
+    uint64_t edges_swept;    /* sum over sweeps of the level's nnz */
+    uint64_t phase0_edges_swept;
+    double phase0_seconds;
+    uint64_t distinct_pairs; /* sum over sweeps of the candidate pairs */
+    double seconds_sweep_kernels; /* device time of the local-move kernels alone */
+    double sweep_bytes;      /* algorithmic bytes of those sweeps: 12E + 24V + 8D each */
+    uint64_t kernel_launches; /* engine kernels launched during the run */
+} mg_summary;
+
+/* Run Louvain to convergence.  Replaces louvain::run / louvain_gl::run /
+ * louvain_baseline::run (src/louvain/louvain.cu:1401-1715). */
+mg_status mg_louvain_run(mg_graph *g, const mg_run_opts *opts /* may be NULL */, mg_result **out);
+mg_status mg_result_summary(const mg_result *r, mg_summary *s);
+/* composed final community of every input vertex (dense ids), n entries */
+mg_status mg_result_assignment(const mg_result *r, uint32_t *out);
+/* vertex count at the start of each phase; *count receives the number */
+mg_status mg_result_level_sizes(const mg_result *r, uint32_t *out, int max, int *count);
+/* the reference's printed table as rows {phase, loop, Q, dQ} */
+mg_status mg_result_trace(const mg_result *r, double *rows4, int max_rows, int *count);
+mg_status mg_result_destroy(mg_result *r);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

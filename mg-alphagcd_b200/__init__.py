@@ -1,0 +1,290 @@
+"""Python front end of the B200 Louvain engine (ctypes over libmgagcd.so).
+
+The engine itself is CUDA C++ behind the C ABI in include/mgagcd.h; this
+module only marshals numpy arrays.  It fails loudly when the shared library
+is missing -- there is no CPU fallback.
+
+The directory name is not a Python identifier; load it with
+``importlib.import_module("mg-alphagcd_b200")`` after putting the repository
+root on ``sys.path``.
+
+Interfaces mirror the reference's stage boundaries (MG-alphaGCD):
+  Graph.from_mtx          -> loadMMSparseMatrix        (src/mmio/mmio_wrapper.cu:297)
+  Graph.bins              -> BIN::bin_create x3         (src/bin/BIN.cu:468-575)
+  Graph.local_move        -> calculate_eicj_and_move_vertex_bin (src/louvain/louvain.cu:1032)
+  Graph.modularity        -> compute_modularity         (src/louvain/louvain.cu:105-238)
+  Graph.coarsen           -> coarsen_graph_mg::coarsen_graph (src/coarsen_graph/coarsen_graph_mg.cu:2054)
+  Graph.louvain           -> louvain::run               (src/louvain/louvain.cu:1401)
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmgagcd.so")
+CLI_PATH = os.path.join(_HERE, "MG_GCD")
+
+MG_OK = 0
+WEIGHT_UNIT, WEIGHT_F32, WEIGHT_F64 = 0, 1, 2
+PREC_FP64, PREC_INT64, PREC_FP32 = 0, 1, 2
+_PREC = {"fp64": PREC_FP64, "int64": PREC_INT64, "fp32": PREC_FP32}
+
+_lib = None
+
+
+class MGError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status
+
+
+class _Opts(ct.Structure):
+    _fields_ = [("device", ct.c_int), ("verbose", ct.c_int), ("hbm_budget_bytes", ct.c_size_t)]
+
+
+class _RunOpts(ct.Structure):
+    _fields_ = [("version", ct.c_int), ("threshold", ct.c_double), ("max_phases", ct.c_int),
+                ("precision", ct.c_int), ("verbose", ct.c_int)]
+
+
+class _Summary(ct.Structure):
+    _fields_ = [("modularity", ct.c_double), ("phases", ct.c_int), ("levels", ct.c_int),
+                ("iterations", ct.c_int), ("communities", ct.c_uint32), ("seconds_total", ct.c_double),
+                ("seconds_local_move", ct.c_double), ("seconds_coarsen", ct.c_double),
+                ("edges_swept", ct.c_uint64), ("phase0_edges_swept", ct.c_uint64),
+                ("phase0_seconds", ct.c_double), ("distinct_pairs", ct.c_uint64),
+                ("seconds_sweep_kernels", ct.c_double), ("sweep_bytes", ct.c_double),
+                ("kernel_launches", ct.c_uint64)]
+
+
+EXPORTED = [
+    "mg_status_string", "mg_version", "mg_init", "mg_destroy", "mg_last_error", "mg_graph_from_csr",
+    "mg_graph_from_device_csr", "mg_graph_from_mtx", "mg_graph_generate_rmat", "mg_graph_generate_sbm",
+    "mg_graph_info", "mg_graph_copy_csr", "mg_graph_destroy", "mg_bins", "mg_bins_offsets", "mg_local_move",
+    "mg_modularity", "mg_coarsen", "mg_louvain_run", "mg_result_summary", "mg_result_assignment",
+    "mg_result_level_sizes", "mg_result_trace", "mg_result_destroy",
+]
+
+
+def lib():
+    """Load libmgagcd.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python mg-alphagcd_b200/build.py` "
+                           "(the engine has no CPU fallback)")
+    L = ct.CDLL(LIB_PATH)
+    vp, u32, u64, i32, dbl = ct.c_void_p, ct.c_uint32, ct.c_uint64, ct.c_int, ct.c_double
+    pp = ct.POINTER(ct.c_void_p)
+    L.mg_status_string.restype = ct.c_char_p
+    L.mg_status_string.argtypes = [i32]
+    L.mg_version.restype = ct.c_char_p
+    L.mg_last_error.restype = ct.c_char_p
+    L.mg_last_error.argtypes = [vp]
+    L.mg_init.argtypes = [pp, ct.POINTER(_Opts)]
+    L.mg_destroy.argtypes = [vp]
+    L.mg_graph_from_csr.argtypes = [vp, u32, vp, vp, vp, i32, pp]
+    L.mg_graph_from_device_csr.argtypes = [vp, u32, u64, vp, vp, vp, i32, pp]
+    L.mg_graph_from_mtx.argtypes = [vp, ct.c_char_p, pp]
+    L.mg_graph_generate_rmat.argtypes = [vp, i32, i32, dbl, dbl, dbl, u64, pp]
+    L.mg_graph_generate_sbm.argtypes = [vp, u32, u32, dbl, dbl, u64, pp]
+    L.mg_graph_info.argtypes = [vp, ct.POINTER(u32), ct.POINTER(u64), ct.POINTER(dbl), ct.POINTER(i32)]
+    L.mg_graph_copy_csr.argtypes = [vp, vp, vp, vp]
+    L.mg_graph_destroy.argtypes = [vp]
+    L.mg_bins.argtypes = [vp, i32, vp, vp, vp, ct.POINTER(u32)]
+    L.mg_bins_offsets.argtypes = [vp, i32, u32, vp, vp, vp, vp, ct.POINTER(u32)]
+    L.mg_local_move.argtypes = [vp, i32, i32, i32, vp, vp, vp, vp, ct.POINTER(u64)]
+    L.mg_modularity.argtypes = [vp, vp, ct.POINTER(dbl)]
+    L.mg_coarsen.argtypes = [vp, vp, vp, pp]
+    L.mg_louvain_run.argtypes = [vp, ct.POINTER(_RunOpts), pp]
+    L.mg_result_summary.argtypes = [vp, ct.POINTER(_Summary)]
+    L.mg_result_assignment.argtypes = [vp, vp]
+    L.mg_result_level_sizes.argtypes = [vp, vp, i32, ct.POINTER(i32)]
+    L.mg_result_trace.argtypes = [vp, vp, i32, ct.POINTER(i32)]
+    L.mg_result_destroy.argtypes = [vp]
+    _lib = L
+    return L
+
+
+def _p(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(ct.c_void_p)
+
+
+class Context:
+    """A CUDA device context of the engine (mg_init / mg_destroy)."""
+
+    def __init__(self, device: int = 0, verbose: bool = False):
+        self.h = ct.c_void_p()
+        opts = _Opts(device, int(verbose), 0)
+        st = lib().mg_init(ct.byref(self.h), ct.byref(opts))
+        if st != MG_OK:
+            raise MGError(st, lib().mg_last_error(None).decode())
+
+    def check(self, st: int, what: str):
+        if st != MG_OK:
+            raise MGError(st, f"{what}: {lib().mg_last_error(self.h).decode()}")
+
+    def close(self):
+        if self.h:
+            lib().mg_destroy(self.h)
+            self.h = ct.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- graph constructors ----------------------------------------------
+    def graph_from_csr(self, n: int, offsets, cols, weights=None) -> "Graph":
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        col = np.ascontiguousarray(cols, dtype=np.uint32)
+        if weights is None:
+            w, wt = None, WEIGHT_UNIT
+        elif np.asarray(weights).dtype == np.float32:
+            w, wt = np.ascontiguousarray(weights, dtype=np.float32), WEIGHT_F32
+        else:
+            w, wt = np.ascontiguousarray(weights, dtype=np.float64), WEIGHT_F64
+        h = ct.c_void_p()
+        self.check(lib().mg_graph_from_csr(self.h, n, _p(off), _p(col), _p(w), wt, ct.byref(h)),
+                   "mg_graph_from_csr")
+        return Graph(self, h)
+
+    def graph_from_mtx(self, path: str) -> "Graph":
+        h = ct.c_void_p()
+        self.check(lib().mg_graph_from_mtx(self.h, path.encode(), ct.byref(h)), "mg_graph_from_mtx")
+        return Graph(self, h)
+
+    def generate_rmat(self, scale: int, edge_factor: int = 16, a=0.57, b=0.19, c=0.19, seed: int = 2) -> "Graph":
+        h = ct.c_void_p()
+        self.check(lib().mg_graph_generate_rmat(self.h, scale, edge_factor, a, b, c, seed, ct.byref(h)),
+                   "mg_graph_generate_rmat")
+        return Graph(self, h)
+
+    def generate_sbm(self, n: int, blocks: int, mean_degree: float = 16.0, intra_frac: float = 0.8,
+                     seed: int = 1) -> "Graph":
+        h = ct.c_void_p()
+        self.check(lib().mg_graph_generate_sbm(self.h, n, blocks, mean_degree, intra_frac, seed, ct.byref(h)),
+                   "mg_graph_generate_sbm")
+        return Graph(self, h)
+
+    def bins_offsets(self, scheme: int, offsets) -> dict:
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        n = len(off) - 1
+        sizes = np.zeros(11, np.uint32)
+        boff = np.zeros(11, np.uint32)
+        perm = np.zeros(max(n, 1), np.uint32)
+        md = ct.c_uint32()
+        self.check(lib().mg_bins_offsets(self.h, scheme, n, _p(off), _p(sizes), _p(boff), _p(perm), ct.byref(md)),
+                   "mg_bins_offsets")
+        nb = {0: 10, 1: 11, 2: 9}[scheme]
+        return {"sizes": sizes[:nb], "offsets": boff[:nb], "perm": perm[:n], "max_degree": int(md.value)}
+
+
+class Graph:
+    """A graph resident in device memory (mg_graph)."""
+
+    def __init__(self, ctx: Context, h: ct.c_void_p):
+        self.ctx = ctx
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().mg_graph_destroy(self.h)
+            self.h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        n, nnz, mass, integ = ct.c_uint32(), ct.c_uint64(), ct.c_double(), ct.c_int()
+        self.ctx.check(lib().mg_graph_info(self.h, ct.byref(n), ct.byref(nnz), ct.byref(mass), ct.byref(integ)),
+                       "mg_graph_info")
+        return {"n": n.value, "nnz": nnz.value, "mass": mass.value, "integral": bool(integ.value)}
+
+    @property
+    def n(self) -> int:
+        return self.info()["n"]
+
+    def csr(self):
+        i = self.info()
+        off = np.zeros(i["n"] + 1, np.uint64)
+        cols = np.zeros(max(i["nnz"], 1), np.uint32)
+        w = np.zeros(max(i["nnz"], 1), np.float64)
+        self.ctx.check(lib().mg_graph_copy_csr(self.h, _p(off), _p(cols), _p(w)), "mg_graph_copy_csr")
+        return off, cols[: i["nnz"]], w[: i["nnz"]]
+
+    def bins(self, scheme: int = 0) -> dict:
+        n = self.info()["n"]
+        sizes = np.zeros(11, np.uint32)
+        boff = np.zeros(11, np.uint32)
+        perm = np.zeros(max(n, 1), np.uint32)
+        md = ct.c_uint32()
+        self.ctx.check(lib().mg_bins(self.h, scheme, _p(sizes), _p(boff), _p(perm), ct.byref(md)), "mg_bins")
+        nb = {0: 10, 1: 11, 2: 9}[scheme]
+        return {"sizes": sizes[:nb], "offsets": boff[:nb], "perm": perm[:n], "max_degree": int(md.value)}
+
+    def local_move(self, C, sigma, k, version: int = 2, up: bool = True, precision: str = "fp64"):
+        n = self.info()["n"]
+        C = np.ascontiguousarray(C, dtype=np.uint32)
+        sigma = np.ascontiguousarray(sigma, dtype=np.float64)
+        k = np.ascontiguousarray(k, dtype=np.float64)
+        out = np.zeros(max(n, 1), np.uint32)
+        d = ct.c_uint64()
+        self.ctx.check(lib().mg_local_move(self.h, version, int(up), _PREC[precision], _p(C), _p(sigma), _p(k),
+                                           _p(out), ct.byref(d)), "mg_local_move")
+        return out[:n], int(d.value)
+
+    def modularity(self, C) -> float:
+        C = np.ascontiguousarray(C, dtype=np.uint32)
+        q = ct.c_double()
+        self.ctx.check(lib().mg_modularity(self.h, _p(C), ct.byref(q)), "mg_modularity")
+        return q.value
+
+    def coarsen(self, C):
+        n = self.info()["n"]
+        C = np.ascontiguousarray(C, dtype=np.uint32)
+        cd = np.zeros(max(n, 1), np.uint32)
+        h = ct.c_void_p()
+        self.ctx.check(lib().mg_coarsen(self.h, _p(C), _p(cd), ct.byref(h)), "mg_coarsen")
+        return cd[:n], Graph(self.ctx, h)
+
+    def louvain(self, version: int = 2, threshold: float = 1e-6, max_phases: int = 1000,
+                precision: str = "fp64", verbose: bool = False) -> dict:
+        opts = _RunOpts(version, threshold, max_phases, _PREC[precision], int(verbose))
+        r = ct.c_void_p()
+        self.ctx.check(lib().mg_louvain_run(self.h, ct.byref(opts), ct.byref(r)), "mg_louvain_run")
+        try:
+            s = _Summary()
+            lib().mg_result_summary(r, ct.byref(s))
+            n = self.info()["n"]
+            a = np.zeros(max(n, 1), np.uint32)
+            lib().mg_result_assignment(r, _p(a))
+            cnt = ct.c_int()
+            lib().mg_result_level_sizes(r, None, 0, ct.byref(cnt))
+            lv = np.zeros(max(cnt.value, 1), np.uint32)
+            lib().mg_result_level_sizes(r, _p(lv), cnt.value, ct.byref(cnt))
+            lib().mg_result_trace(r, None, 0, ct.byref(cnt))
+            tr = np.zeros((max(cnt.value, 1), 4), np.float64)
+            lib().mg_result_trace(r, _p(tr), cnt.value, ct.byref(cnt))
+            out = {f: getattr(s, f) for f, _ in _Summary._fields_}
+            out.update({"assignment": a[:n], "level_sizes": lv[: len(lv) if cnt.value else 0],
+                        "trace": tr[: cnt.value]})
+            out["level_sizes"] = lv[: s.levels]
+            return out
+        finally:
+            lib().mg_result_destroy(r)

@@ -1,0 +1,475 @@
+// capi.cu -- the extern "C" entry points declared in include/mgagcd.h.
+// Every entry point catches engine errors and returns an mg_status; the
+// message of the last failure is kept on the context.
+#include <cstring>
+#include <new>
+
+#include "handles.cuh"
+
+using namespace mg;
+
+namespace {
+
+thread_local std::string g_orphan_error;
+
+mg_status fail(mg_ctx *ctx, mg_status st, const std::string &msg) {
+    if (ctx) ctx->last_error = msg;
+    else g_orphan_error = msg;
+    return st;
+}
+
+template <class F>
+mg_status guarded(mg_ctx *ctx, F &&f) {
+    try {
+        if (ctx) MG_CUDA(cudaSetDevice(ctx->device));
+        f();
+        return MG_OK;
+    } catch (const Error &e) {
+        return fail(ctx, e.status, e.what());
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, MG_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(ctx, MG_ERR_INVALID, e.what());
+    }
+}
+
+__global__ void sigma_from_assignment_kernel(const uint32_t *C, const double *k, uint32_t n, double *sigma) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        atomicAdd(sigma + C[v], k[v]);
+}
+
+// copy a host assignment to the device and check every id is < n
+uint32_t *upload_assignment(mg_ctx *ctx, const uint32_t *C, uint32_t n, DBuf<uint32_t> &buf) {
+    MG_CHECK(C != nullptr || n == 0, MG_ERR_INVALID, "assignment is NULL");
+    for (uint32_t v = 0; v < n; v++) MG_CHECK(C[v] < n, MG_ERR_INVALID, "community id out of range");
+    uint32_t *d = buf.ensure((size_t)n + 1);
+    MG_CUDA(cudaMemcpyAsync(d, C, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+    return d;
+}
+
+}  // namespace
+
+mg_ctx::~mg_ctx() {
+    if (h_acc) cudaFreeHost(h_acc);
+    for (auto &e : ev)
+        if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+namespace mg {
+thread_local unsigned long long g_kernel_launches = 0;
+
+void ctx_prepare(mg_ctx *ctx) {
+    if (ctx->stream) return;
+    MG_CUDA(cudaSetDevice(ctx->device));
+    MG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    MG_CUDA(cudaMallocHost(&ctx->h_acc, sizeof(SweepAcc)));
+    for (auto &e : ctx->ev) MG_CUDA(cudaEventCreate(&e));
+    ctx->mws.init_streams();
+}
+}  // namespace mg
+
+extern "C" {
+
+const char *mg_status_string(mg_status s) {
+    switch (s) {
+        case MG_OK: return "ok";
+        case MG_ERR_INVALID: return "invalid argument";
+        case MG_ERR_CUDA: return "CUDA error";
+        case MG_ERR_OOM: return "out of memory";
+        case MG_ERR_IO: return "I/O error";
+        case MG_ERR_FORMAT: return "malformed input";
+        case MG_ERR_UNSUPPORTED: return "unsupported";
+        case MG_ERR_TIMEOUT: return "device wait timed out";
+        case MG_ERR_CANCELLED: return "cancelled";
+    }
+    return "unknown status";
+}
+
+const char *mg_version(void) { return "mg-alphagcd-b200 0.1 (sm_100a)"; }
+
+mg_status mg_init(mg_ctx **out, const mg_opts *opts) {
+    if (!out) return fail(nullptr, MG_ERR_INVALID, "mg_init: out is NULL");
+    *out = nullptr;
+    mg_ctx *ctx = new (std::nothrow) mg_ctx();
+    if (!ctx) return fail(nullptr, MG_ERR_OOM, "mg_init: host allocation failed");
+    if (opts) {
+        ctx->device = opts->device;
+        ctx->verbose = opts->verbose;
+        ctx->budget = opts->hbm_budget_bytes;
+    }
+    mg_status st = guarded(ctx, [&] {
+        int count = 0;
+        MG_CUDA(cudaGetDeviceCount(&count));
+        MG_CHECK(ctx->device >= 0 && ctx->device < count, MG_ERR_INVALID, "mg_init: no such CUDA device");
+        ctx_prepare(ctx);
+    });
+    if (st != MG_OK) {
+        g_orphan_error = ctx->last_error;
+        delete ctx;
+        return st;
+    }
+    *out = ctx;
+    return MG_OK;
+}
+
+mg_status mg_destroy(mg_ctx *ctx) {
+    if (!ctx) return MG_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    delete ctx;
+    return MG_OK;
+}
+
+const char *mg_last_error(const mg_ctx *ctx) { return ctx ? ctx->last_error.c_str() : g_orphan_error.c_str(); }
+
+// ---- graphs -------------------------------------------------------------------
+
+mg_status mg_graph_from_csr(mg_ctx *ctx, uint32_t n, const uint64_t *offsets, const uint32_t *cols,
+                            const void *weights, int weight_type, mg_graph **out) {
+    if (!ctx || !out) return fail(ctx, MG_ERR_INVALID, "mg_graph_from_csr: NULL argument");
+    *out = nullptr;
+    mg_graph *g = new (std::nothrow) mg_graph();
+    if (!g) return fail(ctx, MG_ERR_OOM, "host allocation failed");
+    g->ctx = ctx;
+    mg_status st = guarded(ctx, [&] { graph_from_host_csr(g, n, offsets, cols, weights, weight_type); });
+    if (st != MG_OK) {
+        delete g;
+        return st;
+    }
+    *out = g;
+    return MG_OK;
+}
+
+mg_status mg_graph_from_device_csr(mg_ctx *ctx, uint32_t n, uint64_t nnz, const uint32_t *d_offsets32,
+                                   const uint32_t *d_cols, const void *d_weights, int weight_type, mg_graph **out) {
+    if (!ctx || !out || !d_offsets32) return fail(ctx, MG_ERR_INVALID, "mg_graph_from_device_csr: NULL argument");
+    *out = nullptr;
+    mg_graph *g = new (std::nothrow) mg_graph();
+    if (!g) return fail(ctx, MG_ERR_OOM, "host allocation failed");
+    g->ctx = ctx;
+    mg_status st = guarded(ctx, [&] { graph_from_device_csr(g, n, nnz, d_offsets32, d_cols, d_weights, weight_type); });
+    if (st != MG_OK) {
+        delete g;
+        return st;
+    }
+    *out = g;
+    return MG_OK;
+}
+
+mg_status mg_graph_from_mtx(mg_ctx *ctx, const char *path, mg_graph **out) {
+    if (!ctx || !out || !path) return fail(ctx, MG_ERR_INVALID, "mg_graph_from_mtx: NULL argument");
+    *out = nullptr;
+    uint32_t n = 0;
+    std::vector<uint64_t> off;
+    std::vector<uint32_t> cols;
+    std::vector<double> w;
+    std::string err;
+    mg_status st;
+    try {
+        st = load_mtx_host(path, n, off, cols, w, err);
+    } catch (const std::bad_alloc &) {
+        return fail(ctx, MG_ERR_OOM, "host allocation failed while loading");
+    }
+    if (st != MG_OK) return fail(ctx, st, "mg_graph_from_mtx: " + err);
+    return mg_graph_from_csr(ctx, n, off.data(), cols.data(), w.data(), MG_WEIGHT_F64, out);
+}
+
+mg_status mg_graph_generate_rmat(mg_ctx *ctx, int scale, int edge_factor, double a, double b, double c, uint64_t seed,
+                                 mg_graph **out) {
+    if (!ctx || !out) return fail(ctx, MG_ERR_INVALID, "mg_graph_generate_rmat: NULL argument");
+    *out = nullptr;
+    mg_graph *g = new (std::nothrow) mg_graph();
+    if (!g) return fail(ctx, MG_ERR_OOM, "host allocation failed");
+    g->ctx = ctx;
+    mg_status st = guarded(ctx, [&] { graph_generate_rmat(g, scale, edge_factor, a, b, c, seed); });
+    if (st != MG_OK) {
+        delete g;
+        return st;
+    }
+    *out = g;
+    return MG_OK;
+}
+
+mg_status mg_graph_generate_sbm(mg_ctx *ctx, uint32_t n, uint32_t blocks, double mean_degree, double intra_frac,
+                                uint64_t seed, mg_graph **out) {
+    if (!ctx || !out) return fail(ctx, MG_ERR_INVALID, "mg_graph_generate_sbm: NULL argument");
+    *out = nullptr;
+    mg_graph *g = new (std::nothrow) mg_graph();
+    if (!g) return fail(ctx, MG_ERR_OOM, "host allocation failed");
+    g->ctx = ctx;
+    mg_status st = guarded(ctx, [&] { graph_generate_sbm(g, n, blocks, mean_degree, intra_frac, seed); });
+    if (st != MG_OK) {
+        delete g;
+        return st;
+    }
+    *out = g;
+    return MG_OK;
+}
+
+mg_status mg_graph_info(const mg_graph *g, uint32_t *n, uint64_t *nnz, double *mass, int *integral) {
+    if (!g) return MG_ERR_INVALID;
+    if (n) *n = g->n;
+    if (nnz) *nnz = g->nnz;
+    if (mass) *mass = g->mass;
+    if (integral) *integral = g->integral;
+    return MG_OK;
+}
+
+mg_status mg_graph_copy_csr(const mg_graph *g, uint64_t *offsets, uint32_t *cols, double *weights) {
+    if (!g) return MG_ERR_INVALID;
+    mg_ctx *ctx = g->ctx;
+    return guarded(ctx, [&] {
+        cudaStream_t s = ctx->stream;
+        if (offsets) {
+            std::vector<uint32_t> o32((size_t)g->n + 1);
+            MG_CUDA(cudaMemcpyAsync(o32.data(), g->off.get(), sizeof(uint32_t) * o32.size(), cudaMemcpyDeviceToHost, s));
+            MG_CUDA(cudaStreamSynchronize(s));
+            for (size_t i = 0; i < o32.size(); i++) offsets[i] = o32[i];
+        }
+        if (cols && g->nnz)
+            MG_CUDA(cudaMemcpyAsync(cols, g->col.get(), sizeof(uint32_t) * g->nnz, cudaMemcpyDeviceToHost, s));
+        if (weights && g->nnz) {
+            if (g->wk == WK_F64) {
+                MG_CUDA(cudaMemcpyAsync(weights, g->w64.get(), sizeof(double) * g->nnz, cudaMemcpyDeviceToHost, s));
+            } else if (g->wk == WK_F32) {
+                std::vector<float> w32(g->nnz);
+                MG_CUDA(cudaMemcpyAsync(w32.data(), g->w32.get(), sizeof(float) * g->nnz, cudaMemcpyDeviceToHost, s));
+                MG_CUDA(cudaStreamSynchronize(s));
+                for (uint64_t e = 0; e < g->nnz; e++) weights[e] = w32[e];
+            } else {
+                for (uint64_t e = 0; e < g->nnz; e++) weights[e] = 1.0;
+            }
+        }
+        MG_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+mg_status mg_graph_destroy(mg_graph *g) {
+    if (!g) return MG_ERR_INVALID;
+    if (g->ctx) cudaSetDevice(g->ctx->device);
+    delete g;
+    return MG_OK;
+}
+
+// ---- stage hooks -----------------------------------------------------------------
+
+mg_status mg_bins(mg_graph *g, int scheme, uint32_t *sizes, uint32_t *offsets, uint32_t *perm, uint32_t *max_degree) {
+    if (!g) return MG_ERR_INVALID;
+    mg_ctx *ctx = g->ctx;
+    return guarded(ctx, [&] {
+        ctx_prepare(ctx);
+        Bins b;
+        uint32_t *d_perm = ctx->tmp32.ensure((size_t)g->n + 1);
+        compute_bins(scheme, g->n, g->off.get(), d_perm, b, ctx->stream, ctx->mws.prim);
+        for (int i = 0; i < 11; i++) {
+            if (sizes) sizes[i] = i < b.count ? b.size[i] : 0;
+            if (offsets) offsets[i] = i < b.count ? b.offset[i] : 0;
+        }
+        if (max_degree) *max_degree = b.max_degree;
+        if (perm && g->n) {
+            MG_CUDA(cudaMemcpyAsync(perm, d_perm, sizeof(uint32_t) * g->n, cudaMemcpyDeviceToHost, ctx->stream));
+            MG_CUDA(cudaStreamSynchronize(ctx->stream));
+        }
+    });
+}
+
+mg_status mg_bins_offsets(mg_ctx *ctx, int scheme, uint32_t n, const uint64_t *offsets, uint32_t *sizes,
+                          uint32_t *bin_offsets, uint32_t *perm, uint32_t *max_degree) {
+    if (!ctx || !offsets) return fail(ctx, MG_ERR_INVALID, "mg_bins_offsets: NULL argument");
+    return guarded(ctx, [&] {
+        ctx_prepare(ctx);
+        std::vector<uint32_t> o32((size_t)n + 1);
+        for (uint32_t i = 0; i <= n; i++) {
+            MG_CHECK(offsets[i] < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "offsets must be below 2^32-1");
+            MG_CHECK(i == 0 || offsets[i] >= offsets[i - 1], MG_ERR_INVALID, "offsets must be non-decreasing");
+            o32[i] = (uint32_t)offsets[i];
+        }
+        DBuf<uint32_t> d_off;
+        uint32_t *d = d_off.ensure((size_t)n + 1);
+        MG_CUDA(cudaMemcpyAsync(d, o32.data(), sizeof(uint32_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, ctx->stream));
+        uint32_t *d_perm = ctx->tmp32.ensure((size_t)n + 1);
+        Bins b;
+        compute_bins(scheme, n, d, d_perm, b, ctx->stream, ctx->mws.prim);
+        for (int i = 0; i < 11; i++) {
+            if (sizes) sizes[i] = i < b.count ? b.size[i] : 0;
+            if (bin_offsets) bin_offsets[i] = i < b.count ? b.offset[i] : 0;
+        }
+        if (max_degree) *max_degree = b.max_degree;
+        if (perm && n) {
+            MG_CUDA(cudaMemcpyAsync(perm, d_perm, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+        }
+        MG_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+mg_status mg_local_move(mg_graph *g, int version, int up, int precision, const uint32_t *C, const double *sigma,
+                        const double *k, uint32_t *C_new, uint64_t *distinct) {
+    if (!g || !C || !sigma || !k || !C_new) return fail(g ? g->ctx : nullptr, MG_ERR_INVALID, "mg_local_move: NULL argument");
+    mg_ctx *ctx = g->ctx;
+    return guarded(ctx, [&] {
+        ctx_prepare(ctx);
+        MG_CHECK(version >= 0 && version <= 2, MG_ERR_INVALID, "version must be 0, 1 or 2");
+        MG_CHECK(precision >= 0 && precision <= 2, MG_ERR_INVALID, "unknown precision");
+        cudaStream_t s = ctx->stream;
+        const uint32_t n = g->n;
+        uint32_t *dC = upload_assignment(ctx, C, n, ctx->C[0]);
+        uint32_t *dN = ctx->C[1].ensure((size_t)n + 1);
+        double *dk = ctx->k.ensure((size_t)n + 1);
+        double *ds = ctx->sigma.ensure((size_t)n + 1);
+        MG_CUDA(cudaMemcpyAsync(dk, k, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        MG_CUDA(cudaMemcpyAsync(ds, sigma, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+        if (n == 0) return;
+        MoveLevel lvl;
+        move_prepare_level(g->view(), lvl, ctx->mws, s);
+        SweepParams sp;
+        sp.version = version == 1 ? 1 : 2;
+        sp.up = up ? 1 : 0;
+        sp.precision = precision;
+        sp.mass = g->mass;
+        sp.integral = g->integral;
+        sweep_reset_acc(ctx->mws, s);
+        move_sweep(g->view(), lvl, ctx->mws, sp, dC, dN, dk, ds, s);
+        MG_CUDA(cudaMemcpyAsync(C_new, dN, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
+        MG_CUDA(cudaMemcpyAsync(ctx->h_acc, ctx->mws.acc.get(), sizeof(SweepAcc), cudaMemcpyDeviceToHost, s));
+        MG_CUDA(cudaStreamSynchronize(s));
+        if (distinct) *distinct = ctx->h_acc->distinct;
+    });
+}
+
+mg_status mg_modularity(mg_graph *g, const uint32_t *C, double *q) {
+    if (!g || !q) return MG_ERR_INVALID;
+    mg_ctx *ctx = g->ctx;
+    return guarded(ctx, [&] {
+        ctx_prepare(ctx);
+        cudaStream_t s = ctx->stream;
+        const uint32_t n = g->n;
+        if (n == 0 || g->mass <= 0) {
+            *q = 0;
+            return;
+        }
+        uint32_t *dC = upload_assignment(ctx, C, n, ctx->C[0]);
+        uint32_t *dI = ctx->C[2].ensure((size_t)n + 1);
+        uint32_t *dN = ctx->C[1].ensure((size_t)n + 1);
+        double *dk = ctx->k.ensure((size_t)n + 1);
+        double *ds = ctx->sigma.ensure((size_t)n + 1);
+        level_init(g->view(), dk, ds, dI, s);
+        MG_CUDA(cudaMemsetAsync(ds, 0, sizeof(double) * n, s));
+        sigma_from_assignment_kernel<<<148 * 8, 256, 0, s>>>(dC, dk, n, ds);
+        MG_LAUNCH_CHECK();
+        MoveLevel lvl;
+        move_prepare_level(g->view(), lvl, ctx->mws, s);
+        SweepParams sp;
+        sp.mass = g->mass;
+        sp.integral = g->integral;
+        sweep_reset_acc(ctx->mws, s);
+        sigma_sumsq(ds, n, g->integral, ctx->mws, s);
+        move_sweep(g->view(), lvl, ctx->mws, sp, dC, dN, dk, ds, s);  // sums the internal weight of C
+        MG_CUDA(cudaMemcpyAsync(ctx->h_acc, ctx->mws.acc.get(), sizeof(SweepAcc), cudaMemcpyDeviceToHost, s));
+        MG_CUDA(cudaStreamSynchronize(s));
+        *q = modularity_from_acc(*ctx->h_acc, g->mass, g->integral);
+    });
+}
+
+mg_status mg_coarsen(mg_graph *g, const uint32_t *C, uint32_t *C_dense, mg_graph **out) {
+    if (!g || !out) return MG_ERR_INVALID;
+    *out = nullptr;
+    mg_ctx *ctx = g->ctx;
+    mg_graph *ng = new (std::nothrow) mg_graph();
+    if (!ng) return fail(ctx, MG_ERR_OOM, "host allocation failed");
+    ng->ctx = ctx;
+    mg_status st = guarded(ctx, [&] {
+        ctx_prepare(ctx);
+        cudaStream_t s = ctx->stream;
+        const uint32_t n = g->n;
+        uint32_t *dC = upload_assignment(ctx, C, n, ctx->C[0]);
+        uint32_t *dCd = ctx->Cd.ensure((size_t)n + 1);
+        uint32_t nn = relabel_dense(dC, n, dCd, ctx->cws, s);
+        LevelGraph lv;
+        coarsen_level(g->view(), dCd, nn, g->integral, lv, ctx->cws, s, nullptr);
+        if (C_dense && n) {
+            MG_CUDA(cudaMemcpyAsync(C_dense, dCd, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
+        }
+        MG_CUDA(cudaStreamSynchronize(s));
+        ng->n = lv.n;
+        ng->nnz = lv.nnz;
+        std::swap(ng->off.p, lv.off.p);
+        std::swap(ng->off.cap, lv.off.cap);
+        std::swap(ng->col.p, lv.col.p);
+        std::swap(ng->col.cap, lv.col.cap);
+        std::swap(ng->w64.p, lv.w.p);
+        std::swap(ng->w64.cap, lv.w.cap);
+        ng->wk = WK_F64;
+        ng->mass = g->mass;
+        ng->integral = g->integral;
+    });
+    if (st != MG_OK) {
+        delete ng;
+        return st;
+    }
+    *out = ng;
+    return MG_OK;
+}
+
+// ---- full Louvain ----------------------------------------------------------------
+
+mg_status mg_louvain_run(mg_graph *g, const mg_run_opts *opts, mg_result **out) {
+    if (!g || !out) return MG_ERR_INVALID;
+    *out = nullptr;
+    mg_ctx *ctx = g->ctx;
+    mg_run_opts o;
+    o.version = 2;
+    o.threshold = 1e-6;
+    o.max_phases = 1000;
+    o.precision = MG_PREC_FP64;
+    o.verbose = 0;
+    if (opts) o = *opts;
+    if (o.version < 0 || o.version > 2) return fail(ctx, MG_ERR_INVALID, "version must be 0, 1 or 2");
+    if (o.precision < 0 || o.precision > 2) return fail(ctx, MG_ERR_INVALID, "unknown precision");
+    mg_result *r = new (std::nothrow) mg_result();
+    if (!r) return fail(ctx, MG_ERR_OOM, "host allocation failed");
+    mg_status st = guarded(ctx, [&] { louvain_run(ctx, g, o, *r); });
+    if (st != MG_OK) {
+        delete r;
+        return st;
+    }
+    *out = r;
+    return MG_OK;
+}
+
+mg_status mg_result_summary(const mg_result *r, mg_summary *s) {
+    if (!r || !s) return MG_ERR_INVALID;
+    *s = r->sum;
+    return MG_OK;
+}
+
+mg_status mg_result_assignment(const mg_result *r, uint32_t *out) {
+    if (!r || !out) return MG_ERR_INVALID;
+    if (r->n0) memcpy(out, r->assignment.data(), sizeof(uint32_t) * r->n0);
+    return MG_OK;
+}
+
+mg_status mg_result_level_sizes(const mg_result *r, uint32_t *out, int max, int *count) {
+    if (!r) return MG_ERR_INVALID;
+    int c = (int)r->level_sizes.size();
+    if (count) *count = c;
+    if (out)
+        for (int i = 0; i < c && i < max; i++) out[i] = r->level_sizes[i];
+    return MG_OK;
+}
+
+mg_status mg_result_trace(const mg_result *r, double *rows4, int max_rows, int *count) {
+    if (!r) return MG_ERR_INVALID;
+    int c = (int)(r->trace.size() / 4);
+    if (count) *count = c;
+    if (rows4)
+        for (int i = 0; i < c && i < max_rows; i++) memcpy(rows4 + 4 * i, r->trace.data() + 4 * i, 4 * sizeof(double));
+    return MG_OK;
+}
+
+mg_status mg_result_destroy(mg_result *r) {
+    if (!r) return MG_ERR_INVALID;
+    delete r;
+    return MG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,329 @@
+// coarsen.cu -- next-level graph from an assignment.
+//
+// Follows coarsen_graph_mg::coarsen_graph (src/coarsen_graph/coarsen_graph_mg.cu:2054-2240):
+//   * dense, order-preserving relabel: flag used ids, scan, C' = scan[C]
+//     (com_size_is_empty_all_range_cuda + InclusiveSum + renew_community_id_all_range_cuda,
+//      :211-226, :267-286, :1330-1363);
+//   * row r of the next level = every neighbour community c of the members of
+//     r (r itself included, which carries the internal weight as a
+//     self-loop) with the summed weight (aggregate_edges_and_weights_*,
+//     :816-1125).
+// The reference builds each row in a hash table (row order = slot order).
+// Here every edge becomes a key (C'[u] << b) | C'[v], the keys are radix
+// sorted and equal keys merged, so rows come out sorted by neighbour
+// community.  For integral weights the merged sums are exact (prefix sums
+// over 64-bit integers); for real weights they are double sums.
+#include <algorithm>
+
+#include "engine.cuh"
+
+namespace mg {
+
+namespace {
+
+__global__ void mark_used_kernel(const uint32_t *C, uint32_t n, uint32_t *flags) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) flags[C[v]] = 1;
+}
+
+__global__ void apply_relabel_kernel(const uint32_t *C, uint32_t n, const uint32_t *newid, uint32_t *Cd) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) Cd[v] = newid[C[v]];
+}
+
+// one warp per row: key = (C'[u] << bc) | C'[v], payload = weight (if any)
+template <int WK>
+__global__ void expand_keys_kernel(const uint32_t *off, const uint32_t *col, const void *w, uint32_t n,
+                                   const uint32_t *Cd, int bc, uint64_t *keys, double *vals) {
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += (gridDim.x * blockDim.x) >> 5) {
+        const uint32_t lo = off[u], hi = off[u + 1];
+        const uint64_t r = (uint64_t)Cd[u] << bc;
+        for (uint32_t e = lo + lane; e < hi; e += 32) {
+            keys[e] = r | Cd[col[e]];
+            if constexpr (WK == WK_F32) vals[e] = (double)((const float *)w)[e];
+            else if constexpr (WK == WK_F64) vals[e] = ((const double *)w)[e];
+        }
+    }
+}
+
+// head[i] = 1 where a run of equal keys starts
+__global__ void run_heads_kernel(const uint64_t *keys, size_t m, uint32_t *head) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x)
+        head[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+}
+
+// compact run heads: ukey[s] = key, ustart[s] = position
+__global__ void compact_runs_kernel(const uint64_t *keys, size_t m, const uint32_t *head, const uint32_t *seg,
+                                    uint64_t *ukey, uint32_t *ustart) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {
+        if (head[i]) {
+            uint32_t s = seg[i];
+            ukey[s] = keys[i];
+            ustart[s] = (uint32_t)i;
+        }
+    }
+}
+
+// cols of the new CSR from the sorted unique keys
+__global__ void emit_cols_kernel(const uint64_t *ukey, uint32_t u, int bc, uint32_t *col) {
+    const uint64_t mask = (1ull << bc) - 1ull;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < u; s += gridDim.x * blockDim.x)
+        col[s] = (uint32_t)(ukey[s] & mask);
+}
+// off[r] = first unique key whose row is >= r (binary search; empty rows allowed)
+__global__ void emit_offsets_kernel(const uint64_t *ukey, uint32_t u, int bc, uint32_t n_rows, uint32_t *off) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r <= n_rows; r += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = u;
+        while (lo < hi) {
+            uint32_t mid = lo + ((hi - lo) >> 1);
+            if ((uint32_t)(ukey[mid] >> bc) < r) lo = mid + 1;
+            else hi = mid;
+        }
+        off[r] = lo;
+    }
+}
+
+void emit_rows(const uint64_t *ukey, uint32_t u, int bc, uint32_t n_rows, uint32_t *off, uint32_t *col,
+               cudaStream_t s);
+
+// run weights as run lengths (unit weights)
+__global__ void run_lengths_kernel(const uint32_t *ustart, uint32_t u, uint32_t m, double *w) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < u; s += gridDim.x * blockDim.x) {
+        uint32_t end = s + 1 < u ? ustart[s + 1] : m;
+        w[s] = (double)(end - ustart[s]);
+    }
+}
+
+// integral weights: exact prefix sums over uint64, run sum = prefix difference
+__global__ void to_u64_kernel(const double *v, size_t m, uint64_t *o) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x)
+        o[i] = (uint64_t)v[i];
+}
+__global__ void run_diff_kernel(const uint32_t *ustart, uint32_t u, uint32_t m, const uint64_t *pre, double *w) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < u; s += gridDim.x * blockDim.x) {
+        uint32_t end = s + 1 < u ? ustart[s + 1] : m;
+        w[s] = (double)(pre[end] - pre[ustart[s]]);
+    }
+}
+
+// real weights: each thread sums 8 consecutive sorted entries run by run and
+// adds each run piece to its run total
+constexpr int kSegItems = 8;
+__global__ void run_sums_kernel(const double *v, size_t m, const uint32_t *seg, const uint32_t *head, double *w) {
+    size_t base = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) * kSegItems;
+    if (base >= m) return;
+    size_t end = base + kSegItems < m ? base + kSegItems : m;
+    uint32_t cur = seg[base] - (head[base] ? 0u : 1u);
+    double acc = 0;
+    for (size_t i = base; i < end; i++) {
+        uint32_t s = seg[i] - (head[i] ? 0u : 1u);
+        if (s != cur) {
+            atomicAdd(w + cur, acc);
+            acc = 0;
+            cur = s;
+        }
+        acc += v[i];
+    }
+    atomicAdd(w + cur, acc);
+}
+
+__global__ void upper_degree_kernel(const uint32_t *off, const uint32_t *Cd, uint32_t n, uint64_t *up) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        atomicAdd((unsigned long long *)up + Cd[v], (unsigned long long)(off[v + 1] - off[v]));
+}
+
+__global__ void pair_keys_kernel(const uint32_t *u, const uint32_t *v, uint64_t m, int bc, uint64_t *keys) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t a = u[i], b = v[i];
+        if (a == b) {
+            keys[2 * i] = 1ull << (2 * bc);
+            keys[2 * i + 1] = 1ull << (2 * bc);
+        } else {
+            keys[2 * i] = ((uint64_t)a << bc) | b;
+            keys[2 * i + 1] = ((uint64_t)b << bc) | a;
+        }
+    }
+}
+
+__global__ void gather_compose_kernel(uint32_t *assign, const uint32_t *map, uint32_t n0) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n0; v += gridDim.x * blockDim.x)
+        assign[v] = map[assign[v]];
+}
+
+__global__ void identity_kernel(uint32_t *C, uint32_t n) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) C[v] = v;
+}
+
+inline unsigned grid_for(uint64_t n, int threads = 256, uint64_t cap = 148ull * 16) {
+    uint64_t g = ceil_div(n, threads);
+    if (g > cap) g = cap;
+    return (unsigned)(g ? g : 1);
+}
+
+void emit_rows(const uint64_t *ukey, uint32_t u, int bc, uint32_t n_rows, uint32_t *off, uint32_t *col,
+               cudaStream_t s) {
+    emit_cols_kernel<<<grid_for(u), 256, 0, s>>>(ukey, u, bc, col);
+    MG_LAUNCH_CHECK();
+    emit_offsets_kernel<<<grid_for((uint64_t)n_rows + 1), 256, 0, s>>>(ukey, u, bc, n_rows, off);
+    MG_LAUNCH_CHECK();
+}
+
+// Sorted unique keys -> CSR (off, col) and per-run starts; returns the count.
+uint32_t unique_runs(const uint64_t *keys, size_t m, int bc, uint32_t n_rows, LevelGraph &out, CoarsenWorkspace &ws,
+                     cudaStream_t s, uint32_t **ustart_out, uint32_t **seg_out, uint32_t **head_out) {
+    uint32_t *head = ws.rowcnt.ensure(m + 1);
+    uint32_t *seg = ws.seg.ensure(m + 1);
+    run_heads_kernel<<<grid_for(m), 256, 0, s>>>(keys, m, head);
+    MG_LAUNCH_CHECK();
+    exclusive_scan<uint32_t>(head, seg, m, seg + m, s, ws.prim);
+    uint32_t u = 0;
+    MG_CUDA(cudaMemcpyAsync(&u, seg + m, sizeof u, cudaMemcpyDeviceToHost, s));
+    MG_CUDA(cudaStreamSynchronize(s));
+    uint64_t *ukey = ws.u64tmp.ensure(u + 1);
+    uint32_t *ustart = ws.u32tmp.ensure(u + 1);
+    compact_runs_kernel<<<grid_for(m), 256, 0, s>>>(keys, m, head, seg, ukey, ustart);
+    MG_LAUNCH_CHECK();
+    out.n = n_rows;
+    out.nnz = u;
+    uint32_t *off = out.off.ensure((size_t)n_rows + 1);
+    uint32_t *col = out.col.ensure(u + 1);
+    if (u == 0) {
+        MG_CUDA(cudaMemsetAsync(off, 0, sizeof(uint32_t) * ((size_t)n_rows + 1), s));
+    } else {
+        emit_rows(ukey, u, bc, n_rows, off, col, s);
+    }
+    *ustart_out = ustart;
+    *seg_out = seg;
+    *head_out = head;
+    return u;
+}
+
+}  // namespace
+
+uint32_t relabel_dense(const uint32_t *C, uint32_t n, uint32_t *C_dense, CoarsenWorkspace &ws, cudaStream_t s) {
+    if (n == 0) return 0;
+    uint32_t *flags = ws.flags.ensure((size_t)n + 1);
+    uint32_t *newid = ws.newid.ensure((size_t)n + 1);
+    MG_CUDA(cudaMemsetAsync(flags, 0, sizeof(uint32_t) * n, s));
+    mark_used_kernel<<<grid_for(n), 256, 0, s>>>(C, n, flags);
+    MG_LAUNCH_CHECK();
+    exclusive_scan<uint32_t>(flags, newid, n, newid + n, s, ws.prim);
+    apply_relabel_kernel<<<grid_for(n), 256, 0, s>>>(C, n, newid, C_dense);
+    MG_LAUNCH_CHECK();
+    uint32_t nn = 0;
+    MG_CUDA(cudaMemcpyAsync(&nn, newid + n, sizeof nn, cudaMemcpyDeviceToHost, s));
+    MG_CUDA(cudaStreamSynchronize(s));
+    return nn;
+}
+
+void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int integral, LevelGraph &out,
+                   CoarsenWorkspace &ws, cudaStream_t s, uint64_t *upper_degree_off) {
+    const size_t m = g.nnz;
+    const int bc = bits_for(n_new);
+    if (upper_degree_off) {
+        MG_CUDA(cudaMemsetAsync(upper_degree_off, 0, sizeof(uint64_t) * ((size_t)n_new + 1), s));
+        upper_degree_kernel<<<grid_for(g.n), 256, 0, s>>>(g.off, Cd, g.n, upper_degree_off);
+        MG_LAUNCH_CHECK();
+        exclusive_scan<uint64_t>(upper_degree_off, upper_degree_off, n_new, upper_degree_off + n_new, s, ws.prim);
+    }
+    if (m == 0) {
+        out.n = n_new;
+        out.nnz = 0;
+        MG_CUDA(cudaMemsetAsync(out.off.ensure((size_t)n_new + 1), 0, sizeof(uint32_t) * ((size_t)n_new + 1), s));
+        out.col.ensure(1);
+        out.w.ensure(1);
+        return;
+    }
+    uint64_t *keys = ws.keys.ensure(m);
+    uint64_t *keys2 = ws.keys_alt.ensure(m);
+    const bool weighted = g.wk != WK_UNIT;
+    double *vals = weighted ? ws.vals.ensure(m + 1) : nullptr;
+    double *vals2 = weighted ? ws.vals_alt.ensure(m + 1) : nullptr;
+    unsigned gw = grid_for((uint64_t)g.n * 32);
+    if (g.wk == WK_UNIT) expand_keys_kernel<WK_UNIT><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, Cd, bc, keys, vals);
+    else if (g.wk == WK_F32) expand_keys_kernel<WK_F32><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, Cd, bc, keys, vals);
+    else expand_keys_kernel<WK_F64><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, Cd, bc, keys, vals);
+    MG_LAUNCH_CHECK();
+    bool flipped;
+    if (weighted) flipped = radix_sort<double>(keys, vals, keys2, vals2, m, 2 * bc, s, ws.prim);
+    else flipped = radix_sort<NoVal>(keys, (NoVal *)nullptr, keys2, (NoVal *)nullptr, m, 2 * bc, s, ws.prim);
+    const uint64_t *sk = flipped ? keys2 : keys;
+    const double *sv = flipped ? vals2 : vals;
+    uint32_t *ustart, *seg, *head;
+    uint32_t u = unique_runs(sk, m, bc, n_new, out, ws, s, &ustart, &seg, &head);
+    double *w = out.w.ensure(u + 1);
+    if (!weighted) {
+        run_lengths_kernel<<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)m, w);
+        MG_LAUNCH_CHECK();
+    } else if (integral) {
+        // exact: 64-bit prefix sums over the sorted weights, run sum = difference
+        uint64_t *pre = (uint64_t *)(flipped ? vals : vals2);
+        to_u64_kernel<<<grid_for(m), 256, 0, s>>>(sv, m, pre);
+        MG_LAUNCH_CHECK();
+        exclusive_scan<uint64_t>(pre, pre, m, pre + m, s, ws.prim);
+        run_diff_kernel<<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)m, pre, w);
+        MG_LAUNCH_CHECK();
+    } else {
+        MG_CUDA(cudaMemsetAsync(w, 0, sizeof(double) * u, s));
+        run_sums_kernel<<<(unsigned)ceil_div(ceil_div(m, kSegItems), 256), 256, 0, s>>>(sv, m, seg, head, w);
+        MG_LAUNCH_CHECK();
+    }
+}
+
+void csr_from_device_pairs(uint32_t n, uint64_t m, const uint32_t *u, const uint32_t *v, LevelGraph &out,
+                           CoarsenWorkspace &ws, cudaStream_t s) {
+    const size_t mm = 2 * m;
+    MG_CHECK(mm < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "graph has more than 2^32-1 directed entries");
+    if (m == 0) {
+        out.n = n;
+        out.nnz = 0;
+        MG_CUDA(cudaMemsetAsync(out.off.ensure((size_t)n + 1), 0, sizeof(uint32_t) * ((size_t)n + 1), s));
+        out.col.ensure(1);
+        return;
+    }
+    const int bc = bits_for(n);
+    uint64_t *keys = ws.keys.ensure(mm + 1);
+    uint64_t *keys2 = ws.keys_alt.ensure(mm + 1);
+    pair_keys_kernel<<<grid_for(m), 256, 0, s>>>(u, v, m, bc, keys);
+    MG_LAUNCH_CHECK();
+    // self-loop markers (bit 2*bc set) sort last and are dropped below
+    bool flipped = radix_sort<NoVal>(keys, (NoVal *)nullptr, keys2, (NoVal *)nullptr, mm, 2 * bc + 1, s, ws.prim);
+    const uint64_t *sk = flipped ? keys2 : keys;
+    uint32_t *head = ws.rowcnt.ensure(mm + 1);
+    uint32_t *seg = ws.seg.ensure(mm + 1);
+    run_heads_kernel<<<grid_for(mm), 256, 0, s>>>(sk, mm, head);
+    MG_LAUNCH_CHECK();
+    exclusive_scan<uint32_t>(head, seg, mm, seg + mm, s, ws.prim);
+    uint32_t nu = 0;
+    uint64_t last = 0;
+    MG_CUDA(cudaMemcpyAsync(&nu, seg + mm, sizeof nu, cudaMemcpyDeviceToHost, s));
+    MG_CUDA(cudaMemcpyAsync(&last, sk + mm - 1, sizeof last, cudaMemcpyDeviceToHost, s));
+    MG_CUDA(cudaStreamSynchronize(s));
+    uint64_t *ukey = ws.u64tmp.ensure((size_t)nu + 1);
+    uint32_t *ustart = ws.u32tmp.ensure((size_t)nu + 1);
+    compact_runs_kernel<<<grid_for(mm), 256, 0, s>>>(sk, mm, head, seg, ukey, ustart);
+    MG_LAUNCH_CHECK();
+    uint32_t uu = nu - (last == (1ull << (2 * bc)) ? 1u : 0u);
+    out.n = n;
+    out.nnz = uu;
+    uint32_t *off = out.off.ensure((size_t)n + 1);
+    uint32_t *col = out.col.ensure((size_t)uu + 1);
+    if (uu == 0) {
+        MG_CUDA(cudaMemsetAsync(off, 0, sizeof(uint32_t) * ((size_t)n + 1), s));
+    } else {
+        emit_rows(ukey, uu, bc, n, off, col, s);
+    }
+}
+
+void gather_compose(uint32_t *assign, const uint32_t *map, uint32_t n0, cudaStream_t s) {
+    if (n0 == 0) return;
+    gather_compose_kernel<<<grid_for(n0), 256, 0, s>>>(assign, map, n0);
+    MG_LAUNCH_CHECK();
+}
+
+void fill_identity(uint32_t *C, uint32_t n, cudaStream_t s) {
+    if (n == 0) return;
+    identity_kernel<<<grid_for(n), 256, 0, s>>>(C, n);
+    MG_LAUNCH_CHECK();
+}
+
+}  // namespace mg

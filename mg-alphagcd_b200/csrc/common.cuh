@@ -1,0 +1,120 @@
+// common.cuh -- shared types, error handling and device helpers of the B200
+// Louvain engine.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/mgagcd.h"
+
+namespace mg {
+
+struct Error : std::runtime_error {
+    mg_status status;
+    Error(mg_status s, const std::string &m) : std::runtime_error(m), status(s) {}
+};
+
+#define MG_STR2(x) #x
+#define MG_STR(x) MG_STR2(x)
+#define MG_CUDA(call)                                                                              \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            throw ::mg::Error(e_ == cudaErrorMemoryAllocation ? MG_ERR_OOM : MG_ERR_CUDA,          \
+                              std::string(#call) + ": " + cudaGetErrorString(e_) +                 \
+                                  " (" __FILE__ ":" MG_STR(__LINE__) ")");                        \
+    } while (0)
+#define MG_CHECK(cond, st, msg)                                                                    \
+    do {                                                                                           \
+        if (!(cond)) throw ::mg::Error((st), (msg));                                               \
+    } while (0)
+// Every kernel launch of the engine is followed by MG_LAUNCH_CHECK(), which
+// also counts the launch (reported per run in mg_summary.kernel_launches).
+extern thread_local unsigned long long g_kernel_launches;
+#define MG_LAUNCH_CHECK()                 \
+    do {                                  \
+        ::mg::g_kernel_launches++;        \
+        MG_CUDA(cudaGetLastError());      \
+    } while (0)
+
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+constexpr int kNumSMs = 148;
+
+enum WeightKind { WK_UNIT = 0, WK_F32 = 1, WK_F64 = 2 };
+
+inline uint64_t ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+inline uint32_t pow2_at_least(uint64_t x, uint32_t lo = 16) {
+    uint32_t p = lo;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+// ---- device buffers ------------------------------------------------------
+// Grow-only device allocation owned by the engine (cudaMalloc on growth only).
+template <class T>
+struct DBuf {
+    T *p = nullptr;
+    size_t cap = 0;
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+    ~DBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    T *ensure(size_t n) {
+        if (n > cap) {
+            release();
+            size_t want = n < 16 ? 16 : n;
+            MG_CUDA(cudaMalloc(&p, want * sizeof(T)));
+            cap = want;
+        }
+        return p;
+    }
+    T *get() const { return p; }
+};
+
+// ---- device helpers ----------------------------------------------------------
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Multiplicative hash onto [0, 2^bits)
+__device__ __forceinline__ uint32_t hash_slot(uint32_t c, int bits) {
+    return (c * 0x9E3779B1u) >> (32 - bits);
+}
+// Multiplicative hash onto [0, size) for arbitrary size
+__device__ __forceinline__ uint32_t hash_range(uint32_t c, uint32_t size) {
+    return (uint32_t)(((uint64_t)(c * 0x9E3779B1u) * size) >> 32);
+}
+
+// splitmix64 finaliser and the counter-based stream built on it; identical to
+// the test oracle's generator so that seeded graphs agree bit for bit.
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__host__ __device__ __forceinline__ uint64_t rng_key(uint64_t seed, uint64_t stream) {
+    return mix64(seed * 0x2545F4914F6CDD1Dull + stream);
+}
+__host__ __device__ __forceinline__ uint64_t rng_at(uint64_t key, uint64_t ctr) {
+    return mix64(key + ctr * 0x9E3779B97F4A7C15ull);
+}
+__host__ __device__ __forceinline__ uint32_t uni32(uint32_t x, uint32_t range) {
+    return (uint32_t)(((uint64_t)x * range) >> 32);
+}
+
+}  // namespace mg

@@ -1,0 +1,292 @@
+// graph.cu -- device graphs: construction from host / device CSR, coarsened
+// levels, and the seeded R-MAT / SBM generators.
+#include <cmath>
+#include <vector>
+
+#include "handles.cuh"
+
+namespace mg {
+
+namespace {
+
+__global__ void rmat_pairs_kernel(int scale, uint64_t m, uint64_t t1, uint64_t t2, uint64_t t3, uint64_t key,
+                                  uint32_t *u, uint32_t *v) {
+    const int words = (scale + 1) / 2;
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t uu = 0, vv = 0;
+        for (int wi = 0; wi < words; wi++) {
+            uint64_t r = rng_at(key, k * (uint64_t)words + (uint64_t)wi);
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                int l = 2 * wi + h;
+                if (l >= scale) break;
+                uint64_t x = h ? (r >> 32) : (r & 0xFFFFFFFFull);
+                uint32_t bu, bv;
+                if (x < t1) { bu = 0; bv = 0; }
+                else if (x < t2) { bu = 0; bv = 1; }
+                else if (x < t3) { bu = 1; bv = 0; }
+                else { bu = 1; bv = 1; }
+                uu |= bu << (scale - 1 - l);
+                vv |= bv << (scale - 1 - l);
+            }
+        }
+        u[k] = uu;
+        v[k] = vv;
+    }
+}
+
+__global__ void sbm_pairs_kernel(uint32_t n, uint32_t blocks, uint64_t min_, uint64_t m, uint64_t kin, uint64_t kout,
+                                 uint32_t *u, uint32_t *v) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (uint64_t)gridDim.x * blockDim.x) {
+        if (k < min_) {
+            uint64_t r0 = rng_at(kin, 2 * k), r1 = rng_at(kin, 2 * k + 1);
+            uint32_t bb = uni32((uint32_t)r0, blocks);
+            uint32_t lo = (uint32_t)((uint64_t)bb * n / blocks), hi = (uint32_t)((uint64_t)(bb + 1) * n / blocks);
+            u[k] = lo + uni32((uint32_t)(r0 >> 32), hi - lo);
+            v[k] = lo + uni32((uint32_t)r1, hi - lo);
+        } else {
+            uint64_t j = k - min_;
+            uint64_t r0 = rng_at(kout, 2 * j), r1 = rng_at(kout, 2 * j + 1);
+            uint32_t b1 = uni32((uint32_t)r0, blocks);
+            uint32_t b2 = uni32((uint32_t)(r0 >> 32), blocks - 1);
+            if (b2 >= b1) b2++;
+            uint32_t lo1 = (uint32_t)((uint64_t)b1 * n / blocks), hi1 = (uint32_t)((uint64_t)(b1 + 1) * n / blocks);
+            uint32_t lo2 = (uint32_t)((uint64_t)b2 * n / blocks), hi2 = (uint32_t)((uint64_t)(b2 + 1) * n / blocks);
+            u[k] = lo1 + uni32((uint32_t)r1, hi1 - lo1);
+            v[k] = lo2 + uni32((uint32_t)(r1 >> 32), hi2 - lo2);
+        }
+    }
+}
+
+// 64-bit offsets -> 32-bit; flags non-monotone offsets (bit 0) and column ids
+// out of range (bit 1)
+__global__ void check_csr_kernel(const uint64_t *off64, uint32_t n, const uint32_t *cols, uint64_t nnz,
+                                 uint32_t *off32, int *bad) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    int b = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += stride) {
+        uint64_t o = off64[i];
+        off32[i] = (uint32_t)o;
+        if (i > 0 && o < off64[i - 1]) b |= 1;
+    }
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nnz; e += stride)
+        if (cols[e] >= n) b |= 2;
+    if (b) atomicOr(bad, b);
+}
+
+// per-block partial sums of weights and integrality flags
+template <class T>
+__global__ void weight_stats_kernel(const T *w, uint64_t m, double *partial, int *nonintegral, int *nonunit) {
+    double s = 0;
+    int ni = 0, nu = 0;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m; e += (uint64_t)gridDim.x * blockDim.x) {
+        double x = (double)w[e];
+        s += x;
+        ni |= (x < 0 || x != floor(x));
+        nu |= (x != 1.0);
+    }
+    s = warp_sum(s);
+    __shared__ double red[32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    if (__any_sync(0xffffffffu, ni) && (threadIdx.x & 31) == 0) atomicOr(nonintegral, 1);
+    if (__any_sync(0xffffffffu, nu) && (threadIdx.x & 31) == 0) atomicOr(nonunit, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) t += red[i];
+        partial[blockIdx.x] = t;
+    }
+}
+
+}  // namespace
+
+// mass and integrality of a device weight array (deterministic block order)
+template <class T>
+static void device_weight_stats(const T *w, uint64_t m, double &mass, int &integral, int &unit, cudaStream_t s) {
+    const unsigned blocks = 148 * 4;
+    DBuf<double> part;
+    DBuf<int> flags;
+    double *p = part.ensure(blocks);
+    int *f = flags.ensure(2);
+    MG_CUDA(cudaMemsetAsync(f, 0, 2 * sizeof(int), s));
+    weight_stats_kernel<T><<<blocks, 256, 0, s>>>(w, m, p, f, f + 1);
+    MG_LAUNCH_CHECK();
+    std::vector<double> hp(blocks);
+    int hf[2];
+    MG_CUDA(cudaMemcpyAsync(hp.data(), p, blocks * sizeof(double), cudaMemcpyDeviceToHost, s));
+    MG_CUDA(cudaMemcpyAsync(hf, f, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    MG_CUDA(cudaStreamSynchronize(s));
+    double t = 0;
+    for (double x : hp) t += x;
+    mass = t;
+    integral = !hf[0] && t < 4294967296.0;
+    unit = !hf[1];
+}
+
+void graph_from_host_csr(mg_graph *g, uint32_t n, const uint64_t *offsets, const uint32_t *cols, const void *w,
+                         int weight_type) {
+    MG_CHECK(offsets != nullptr, MG_ERR_INVALID, "offsets is NULL");
+    MG_CHECK(n < 0xFFFFFFFFu, MG_ERR_UNSUPPORTED, "too many vertices");
+    MG_CHECK(offsets[0] == 0, MG_ERR_INVALID, "offsets[0] must be 0");
+    const uint64_t nnz = offsets[n];
+    MG_CHECK(nnz < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "nnz must be below 2^32-1");
+    MG_CHECK(nnz == 0 || cols != nullptr, MG_ERR_INVALID, "cols is NULL");
+    MG_CHECK(weight_type >= MG_WEIGHT_UNIT && weight_type <= MG_WEIGHT_F64, MG_ERR_INVALID, "bad weight type");
+    MG_CHECK(weight_type == MG_WEIGHT_UNIT || nnz == 0 || w != nullptr, MG_ERR_INVALID, "weights is NULL");
+    // mass in CSR order (src/graph/host_graph.cpp:112-115), integrality, unit detection
+    double mass = (double)nnz;
+    bool nonint = false, unit = true;
+    if (weight_type != MG_WEIGHT_UNIT) {
+        mass = 0;
+        for (uint64_t e = 0; e < nnz; e++) {
+            double x = weight_type == MG_WEIGHT_F32 ? (double)((const float *)w)[e] : ((const double *)w)[e];
+            mass += x;
+            nonint |= (x < 0 || x != std::floor(x));
+            unit &= (x == 1.0);
+        }
+    }
+    cudaStream_t s = g->ctx->stream;
+    g->n = n;
+    g->nnz = nnz;
+    // offsets and columns are checked on the device after the copy
+    {
+        DBuf<uint64_t> off64;
+        DBuf<int> bad;
+        uint64_t *d64 = off64.ensure((size_t)n + 1);
+        int *dbad = bad.ensure(1);
+        MG_CUDA(cudaMemsetAsync(dbad, 0, sizeof(int), s));
+        MG_CUDA(cudaMemcpyAsync(d64, offsets, sizeof(uint64_t) * ((size_t)n + 1), cudaMemcpyHostToDevice, s));
+        uint32_t *doff = g->off.ensure((size_t)n + 1);
+        uint32_t *dcol = g->col.ensure(nnz + 1);
+        MG_CUDA(cudaMemcpyAsync(dcol, cols, sizeof(uint32_t) * nnz, cudaMemcpyHostToDevice, s));
+        check_csr_kernel<<<148 * 8, 256, 0, s>>>(d64, n, dcol, nnz, doff, dbad);
+        MG_LAUNCH_CHECK();
+        int hbad = 0;
+        MG_CUDA(cudaMemcpyAsync(&hbad, dbad, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MG_CUDA(cudaStreamSynchronize(s));
+        MG_CHECK(!(hbad & 1), MG_ERR_INVALID, "offsets must be non-decreasing");
+        MG_CHECK(!(hbad & 2), MG_ERR_INVALID, "column index out of range");
+    }
+    if (unit) {
+        g->wk = WK_UNIT;
+    } else if (weight_type == MG_WEIGHT_F32) {
+        g->wk = WK_F32;
+        MG_CUDA(cudaMemcpyAsync(g->w32.ensure(nnz + 1), w, sizeof(float) * nnz, cudaMemcpyHostToDevice, s));
+    } else {
+        g->wk = WK_F64;
+        MG_CUDA(cudaMemcpyAsync(g->w64.ensure(nnz + 1), w, sizeof(double) * nnz, cudaMemcpyHostToDevice, s));
+    }
+    g->mass = mass;
+    g->integral = !nonint && mass < 4294967296.0;
+    MG_CUDA(cudaStreamSynchronize(s));
+}
+
+void graph_from_device_csr(mg_graph *g, uint32_t n, uint64_t nnz, const uint32_t *d_off, const uint32_t *d_cols,
+                           const void *d_w, int weight_type) {
+    MG_CHECK(nnz < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "nnz must be below 2^32-1");
+    cudaStream_t s = g->ctx->stream;
+    g->n = n;
+    g->nnz = nnz;
+    MG_CUDA(cudaMemcpyAsync(g->off.ensure((size_t)n + 1), d_off, sizeof(uint32_t) * ((size_t)n + 1),
+                            cudaMemcpyDeviceToDevice, s));
+    MG_CUDA(cudaMemcpyAsync(g->col.ensure(nnz + 1), d_cols, sizeof(uint32_t) * nnz, cudaMemcpyDeviceToDevice, s));
+    g->wk = WK_UNIT;
+    g->mass = (double)nnz;
+    g->integral = nnz < 4294967296ull;
+    if (weight_type != MG_WEIGHT_UNIT && nnz > 0) {
+        int integral = 0, unit = 0;
+        if (weight_type == MG_WEIGHT_F32) {
+            device_weight_stats<float>((const float *)d_w, nnz, g->mass, integral, unit, s);
+            if (!unit) {
+                g->wk = WK_F32;
+                MG_CUDA(cudaMemcpyAsync(g->w32.ensure(nnz + 1), d_w, sizeof(float) * nnz, cudaMemcpyDeviceToDevice, s));
+            }
+        } else {
+            device_weight_stats<double>((const double *)d_w, nnz, g->mass, integral, unit, s);
+            if (!unit) {
+                g->wk = WK_F64;
+                MG_CUDA(cudaMemcpyAsync(g->w64.ensure(nnz + 1), d_w, sizeof(double) * nnz, cudaMemcpyDeviceToDevice, s));
+            }
+        }
+        g->integral = integral;
+    }
+    MG_CUDA(cudaStreamSynchronize(s));
+}
+
+void graph_from_level(mg_graph *g, LevelGraph &lv, int integral, double mass) {
+    cudaStream_t s = g->ctx->stream;
+    g->n = lv.n;
+    g->nnz = lv.nnz;
+    MG_CUDA(cudaMemcpyAsync(g->off.ensure((size_t)lv.n + 1), lv.off.get(), sizeof(uint32_t) * ((size_t)lv.n + 1),
+                            cudaMemcpyDeviceToDevice, s));
+    MG_CUDA(cudaMemcpyAsync(g->col.ensure(lv.nnz + 1), lv.col.get(), sizeof(uint32_t) * lv.nnz,
+                            cudaMemcpyDeviceToDevice, s));
+    MG_CUDA(cudaMemcpyAsync(g->w64.ensure(lv.nnz + 1), lv.w.get(), sizeof(double) * lv.nnz,
+                            cudaMemcpyDeviceToDevice, s));
+    g->wk = WK_F64;
+    g->integral = integral;
+    g->mass = mass;
+    MG_CUDA(cudaStreamSynchronize(s));
+}
+
+static void finish_generated(mg_graph *g, uint32_t n, uint64_t m, DBuf<uint32_t> &u, DBuf<uint32_t> &v) {
+    mg_ctx *ctx = g->ctx;
+    cudaStream_t s = ctx->stream;
+    LevelGraph lv;
+    csr_from_device_pairs(n, m, u.get(), v.get(), lv, ctx->cws, s);
+    u.release();
+    v.release();
+    g->n = n;
+    g->nnz = lv.nnz;
+    // adopt the level's buffers
+    std::swap(g->off.p, lv.off.p);
+    std::swap(g->off.cap, lv.off.cap);
+    std::swap(g->col.p, lv.col.p);
+    std::swap(g->col.cap, lv.col.cap);
+    g->wk = WK_UNIT;
+    g->mass = (double)lv.nnz;
+    g->integral = lv.nnz < 4294967296ull;
+    MG_CUDA(cudaStreamSynchronize(s));
+}
+
+void graph_generate_rmat(mg_graph *g, int scale, int edge_factor, double a, double b, double c, uint64_t seed) {
+    MG_CHECK(scale >= 1 && scale <= 31 && edge_factor >= 1, MG_ERR_INVALID, "rmat: bad scale or edge factor");
+    MG_CHECK(a >= 0 && b >= 0 && c >= 0 && a + b + c <= 1.0, MG_ERR_INVALID, "rmat: bad probabilities");
+    const uint32_t n = 1u << scale;
+    const uint64_t m = (uint64_t)edge_factor << scale;
+    MG_CHECK(2 * m < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "rmat: more than 2^32-1 directed entries");
+    const uint64_t t1 = (uint64_t)(a * 4294967296.0);
+    const uint64_t t2 = (uint64_t)((a + b) * 4294967296.0);
+    const uint64_t t3 = (uint64_t)((a + b + c) * 4294967296.0);
+    const uint64_t key = rng_key(seed, 0x524d4154ull);
+    DBuf<uint32_t> u, v;
+    u.ensure(m);
+    v.ensure(m);
+    cudaStream_t s = g->ctx->stream;
+    rmat_pairs_kernel<<<148 * 16, 256, 0, s>>>(scale, m, t1, t2, t3, key, u.get(), v.get());
+    MG_LAUNCH_CHECK();
+    finish_generated(g, n, m, u, v);
+}
+
+void graph_generate_sbm(mg_graph *g, uint32_t n, uint32_t blocks, double mean_degree, double intra_frac,
+                        uint64_t seed) {
+    MG_CHECK(blocks >= 1 && n >= blocks && n < 0xFFFFFFFFu, MG_ERR_INVALID, "sbm: need 1 <= blocks <= n");
+    const double din = mean_degree * intra_frac;
+    const double dout = mean_degree - din;
+    const uint64_t min_ = (uint64_t)std::llround((double)n * din / 2.0);
+    const uint64_t mout = blocks > 1 ? (uint64_t)std::llround((double)n * dout / 2.0) : 0;
+    const uint64_t m = min_ + mout;
+    MG_CHECK(2 * m < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "sbm: more than 2^32-1 directed entries");
+    DBuf<uint32_t> u, v;
+    u.ensure(m + 1);
+    v.ensure(m + 1);
+    cudaStream_t s = g->ctx->stream;
+    if (m > 0) {
+        sbm_pairs_kernel<<<148 * 16, 256, 0, s>>>(n, blocks, min_, m, rng_key(seed, 0x53424d31ull),
+                                                  rng_key(seed, 0x53424d32ull), u.get(), v.get());
+        MG_LAUNCH_CHECK();
+    }
+    finish_generated(g, n, m, u, v);
+}
+
+}  // namespace mg

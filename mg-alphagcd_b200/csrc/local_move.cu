@@ -1,0 +1,888 @@
+// local_move.cu -- one Louvain local-move sweep on sm_100a.
+//
+// Semantics (identical arithmetic to the reference kernels
+// calculate_eicj_and_move_vertex_sh_tile / _sh_bk / _gl_bk,
+// src/louvain/louvain.cu:404-1030, and the version-1 variants in
+// src/louvain/louvain_gl.cu:504,578):
+//   for vertex i with src = P[i], a = sigma[src] - k_i:
+//     every edge (i,j,w), c = P[j]:  c != src -> k_ic += w ;  c == src, j != i -> e += w
+//     gain_c = (k_ic - (e - k_i*(a - sigma[c])/(2m))) / m      (m = mass/2)
+//     best starts at (0, src); a candidate wins on a larger gain, or on an
+//     equal gain with a smaller id (up sweep) / larger id (down sweep);
+//     version 2 clamps the result to min/max(dst, src); version 1 only lets
+//     communities below (up) / above (down) src compete.
+// The comparison is a total order, so the winner does not depend on the order
+// in which candidates are visited.
+//
+// Kernel shapes (bins from the reference's 10-bin scheme, src/bin/BIN.cu:72-92):
+//   bins 0-4 (deg <= 2..32): T-lane tiles, one edge per lane; neighbours in the
+//     same community are merged with __match_any_sync, sums over the matching
+//     lanes, a T-wide shuffle argmax.  No hash table at all.
+//   bins 5-8 (deg <= 128..4094): one warp / CTA per vertex with a shared-memory
+//     open-addressing table of >= 2*deg slots (load <= 1/2), self-cleaning.
+//   bin 9 (deg > 4094): load-balanced over many CTAs per vertex; global
+//     tables of 2*deg slots (resident in L2 while a vertex is being worked on),
+//     insert items (vertex, 4096-edge chunk), evaluate items (vertex, slot
+//     chunk) and a per-vertex reduction of the chunk winners.
+// Each sweep also accumulates sum_in(P) = sum of weights of edges inside a
+// community of P (self-loops included), the first term of the modularity of P
+// (src/louvain/louvain.cu:105-238), so a separate modularity pass over the
+// edges is not needed.
+#include <algorithm>
+
+#include "engine.cuh"
+
+namespace mg {
+
+namespace {
+
+struct LMArgs {
+    const uint32_t *__restrict__ off;
+    const uint32_t *__restrict__ col;
+    const void *__restrict__ w;
+    const uint32_t *__restrict__ P;
+    uint32_t *__restrict__ N;
+    const double *__restrict__ k;
+    const double *__restrict__ sigma;
+    const uint32_t *__restrict__ perm;
+    double m;            // mass / 2
+    float m_f;
+    long long mass_i;    // mass (integral graphs)
+    int up;
+    int integral;
+    SweepAcc *acc;
+};
+
+template <int WK>
+__device__ __forceinline__ double wload(const void *w, uint32_t e) {
+    if constexpr (WK == WK_UNIT) return 1.0;
+    else if constexpr (WK == WK_F32) return (double)__ldg((const float *)w + e);
+    else return __ldg((const double *)w + e);
+}
+
+// ---- gain in the three precision modes -------------------------------------
+template <int PREC>
+struct Prec;
+template <>
+struct Prec<MG_PREC_FP64> {
+    using G = double;
+    // (k_ic - (e - k_i*(a - s_c)/(2m))) / m, each operation rounded as written
+    __device__ static __forceinline__ G gain(double kic, double e, double ki, double a, double sc,
+                                             const LMArgs &A) {
+        double t = __dmul_rn(ki, __dsub_rn(a, sc));
+        t = __ddiv_rn(t, __dmul_rn(2.0, A.m));
+        t = __dsub_rn(e, t);
+        return __ddiv_rn(__dsub_rn(kic, t), A.m);
+    }
+};
+template <>
+struct Prec<MG_PREC_FP32> {
+    using G = float;
+    __device__ static __forceinline__ G gain(double kic, double e, double ki, double a, double sc,
+                                             const LMArgs &A) {
+        float t = __fmul_rn((float)ki, __fsub_rn((float)a, (float)sc));
+        t = __fdiv_rn(t, __fmul_rn(2.0f, A.m_f));
+        t = __fsub_rn((float)e, t);
+        return __fdiv_rn(__fsub_rn((float)kic, t), A.m_f);
+    }
+};
+template <>
+struct Prec<MG_PREC_INT64> {
+    using G = long long;
+    // 2m*m*gain = 2m*(k_ic - e) + k_i*(a - s_c), exact for integral weights
+    __device__ static __forceinline__ G gain(double kic, double e, double ki, double a, double sc,
+                                             const LMArgs &A) {
+        return A.mass_i * ((long long)kic - (long long)e) + (long long)ki * ((long long)a - (long long)sc);
+    }
+};
+
+template <class G>
+__device__ __forceinline__ bool better(G g2, uint32_t c2, G g1, uint32_t c1, int up) {
+    return g2 > g1 || (g2 == g1 && (up ? c2 < c1 : c2 > c1));
+}
+
+template <int VER>
+__device__ __forceinline__ bool is_candidate(uint32_t c, uint32_t src, int up) {
+    if constexpr (VER == 1) return up ? c < src : c > src;
+    else return c != src;
+}
+
+template <int VER>
+__device__ __forceinline__ uint32_t final_choice(uint32_t dst, uint32_t src, int up) {
+    if constexpr (VER == 1) return dst;
+    else return up ? (dst < src ? dst : src) : (dst > src ? dst : src);
+}
+
+template <class G>
+__device__ __forceinline__ G shfl_xor_g(G v, int o) {
+    return __shfl_xor_sync(0xffffffffu, v, o);
+}
+
+// Block-level accumulation of sum_in / distinct into the sweep accumulators.
+__device__ __forceinline__ void flush_acc(SweepAcc *acc, int integral, double sin, unsigned dcnt) {
+    __shared__ double s_f;
+    __shared__ unsigned long long s_d;
+    if (threadIdx.x == 0) {
+        s_f = 0;
+        s_d = 0;
+    }
+    __syncthreads();
+    double v = warp_sum(sin);
+    unsigned long long d = warp_sum((unsigned long long)dcnt);
+    if ((threadIdx.x & 31) == 0) {
+        if (v != 0) atomicAdd(&s_f, v);
+        if (d) atomicAdd(&s_d, d);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (integral) {
+            if (s_f != 0) atomicAdd(&acc->sin_u, (unsigned long long)s_f);
+        } else if (s_f != 0) {
+            atomicAdd(&acc->sin_f, s_f);
+        }
+        if (s_d) atomicAdd(&acc->distinct, s_d);
+    }
+}
+
+// ============================================================================
+// bins 0-4: T lanes per vertex, deg <= T
+// ============================================================================
+template <int T, int WK, int PREC, int VER>
+__global__ void __launch_bounds__(256) lm_tile_kernel(LMArgs A, uint32_t bin_off, uint32_t bin_size) {
+    using G = typename Prec<PREC>::G;
+    __shared__ double wbuf[8][32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t gl = lane & (T - 1), gbase = lane & ~(uint32_t)(T - 1);
+    const uint32_t gmask = T == 32 ? 0xffffffffu : (((1u << T) - 1u) << gbase);
+    constexpr uint32_t GPW = 32 / T;
+    double sin = 0;
+    unsigned dcnt = 0;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarp = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t wb = gwarp * GPW; wb < bin_size; wb += nwarp * GPW) {
+        const uint32_t idx = wb + lane / T;
+        const bool active = idx < bin_size;
+        uint32_t i = 0, src = 0, lo = 0, hi = 0;
+        double ki = 0, a = 0;
+        if (active) {
+            i = A.perm[bin_off + idx];
+            lo = A.off[i];
+            hi = A.off[i + 1];
+            src = A.P[i];
+        }
+        const uint32_t e = lo + gl;
+        const bool has = active && e < hi;
+        uint32_t j = kEmpty, c = kEmpty;
+        double w = 0;
+        if (has) {
+            j = __ldg(A.col + e);
+            w = wload<WK>(A.w, e);
+            c = A.P[j];
+        }
+        if (active) {
+            ki = A.k[i];
+            a = A.sigma[src] - ki;
+        }
+        const bool self = has && j == i;
+        const bool inner = has && !self && c == src;
+        const bool cand = has && c != src && is_candidate<VER>(c, src, A.up);
+        const uint32_t key = cand ? c : kEmpty;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key) & gmask;
+        const bool leader = cand && (uint32_t)(__ffs(peers) - 1) == lane;
+        double kic, e_src, selfw;
+        if constexpr (WK == WK_UNIT) {
+            kic = (double)__popc(peers);
+            e_src = (double)__popc(__ballot_sync(0xffffffffu, inner) & gmask);
+            selfw = (double)__popc(__ballot_sync(0xffffffffu, self) & gmask);
+        } else {
+            wbuf[warp][lane] = w;
+            __syncwarp();
+            kic = 0;
+            if (leader) {
+                uint32_t mset = peers;
+                while (mset) {
+                    int l = __ffs(mset) - 1;
+                    kic += wbuf[warp][l];
+                    mset &= mset - 1;
+                }
+            }
+            __syncwarp();
+            e_src = inner ? w : 0.0;
+            selfw = self ? w : 0.0;
+#pragma unroll
+            for (int o = T / 2; o > 0; o >>= 1) {
+                e_src += __shfl_xor_sync(0xffffffffu, e_src, o);
+                selfw += __shfl_xor_sync(0xffffffffu, selfw, o);
+            }
+        }
+        G best = G(0);
+        uint32_t dst = src;
+        if (leader) {
+            G g = Prec<PREC>::gain(kic, e_src, ki, a, A.sigma[c], A);
+            if (better(g, c, best, dst, A.up)) {
+                best = g;
+                dst = c;
+            }
+            dcnt++;
+        }
+#pragma unroll
+        for (int o = T / 2; o > 0; o >>= 1) {
+            G g2 = shfl_xor_g(best, o);
+            uint32_t c2 = __shfl_xor_sync(0xffffffffu, dst, o);
+            if (better(g2, c2, best, dst, A.up)) {
+                best = g2;
+                dst = c2;
+            }
+        }
+        if (active && gl == 0) {
+            A.N[i] = final_choice<VER>(dst, src, A.up);
+            sin += e_src + selfw;
+        }
+    }
+    flush_acc(A.acc, A.integral, sin, dcnt);
+}
+
+// ============================================================================
+// bins 5-8: GT threads per vertex, SLOTS-entry shared table
+// ============================================================================
+template <int WK>
+struct ValT {
+    using type = double;
+};
+template <>
+struct ValT<WK_UNIT> {
+    using type = uint32_t;
+};
+
+template <int GT>
+__device__ __forceinline__ void group_sync() {
+    if constexpr (GT == 32) __syncwarp();
+    else __syncthreads();
+}
+
+// Sum over a group of GT threads; result valid in every thread.
+template <int GT>
+__device__ __forceinline__ double group_sum(double v, double *red) {
+    v = warp_sum(v);
+    if constexpr (GT == 32) {
+        return v;
+    } else {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (lane == 0) red[warp] = v;
+        __syncthreads();
+        double t = 0;
+#pragma unroll
+        for (int w2 = 0; w2 < GT / 32; w2++) t += red[w2];
+        __syncthreads();
+        return t;
+    }
+}
+
+template <int GT, class G>
+__device__ __forceinline__ void group_argmax(G &best, uint32_t &dst, int up, G *rg, uint32_t *rc) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        G g2 = shfl_xor_g(best, o);
+        uint32_t c2 = __shfl_xor_sync(0xffffffffu, dst, o);
+        if (better(g2, c2, best, dst, up)) {
+            best = g2;
+            dst = c2;
+        }
+    }
+    if constexpr (GT > 32) {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (lane == 0) {
+            rg[warp] = best;
+            rc[warp] = dst;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int w2 = 0; w2 < GT / 32; w2++) {
+            if (better(rg[w2], rc[w2], best, dst, up)) {
+                best = rg[w2];
+                dst = rc[w2];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <int X>
+struct Log2 {
+    static constexpr int value = 1 + Log2<X / 2>::value;
+};
+template <>
+struct Log2<1> {
+    static constexpr int value = 0;
+};
+
+template <int SLOTS>
+__device__ __forceinline__ uint32_t table_find_or_insert(uint32_t *keys, uint32_t c) {
+    constexpr int bits = Log2<SLOTS>::value;
+    uint32_t h = hash_slot(c, bits);
+    for (int p = 0; p < SLOTS; p++) {
+        uint32_t cur = ((volatile uint32_t *)keys)[h];
+        if (cur == c) return h;
+        if (cur == kEmpty) {
+            uint32_t prev = atomicCAS(keys + h, kEmpty, c);
+            if (prev == kEmpty || prev == c) return h;
+        }
+        h = (h + 1) & (SLOTS - 1);
+    }
+    return kEmpty;  // unreachable: tables hold >= 2*deg slots
+}
+
+template <int GT, int SLOTS, int WK, int PREC, int VER, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) lm_hash_kernel(LMArgs A, uint32_t bin_off, uint32_t bin_size) {
+    using G = typename Prec<PREC>::G;
+    using V = typename ValT<WK>::type;
+    constexpr int GPB = BLOCK / GT;
+    constexpr int BATCH = 4;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t *keys_all = (uint32_t *)smem_raw;
+    V *vals_all = (V *)(smem_raw + sizeof(uint32_t) * SLOTS * GPB);
+    __shared__ double red_d[32];
+    __shared__ G red_g[32];
+    __shared__ uint32_t red_c[32];
+    const int g = threadIdx.x / GT, t = threadIdx.x % GT;
+    uint32_t *keys = keys_all + g * SLOTS;
+    V *vals = vals_all + g * SLOTS;
+    for (int s2 = threadIdx.x; s2 < SLOTS * GPB; s2 += BLOCK) {
+        keys_all[s2] = kEmpty;
+        vals_all[s2] = V(0);
+    }
+    __syncthreads();
+    double sin = 0;
+    unsigned dcnt = 0;
+    for (uint32_t idx = blockIdx.x * GPB + g; idx - g < bin_size; idx += gridDim.x * GPB) {
+        // the loop condition is uniform inside a group (GT == 32) or block (GT > 32)
+        const bool active = idx < bin_size;
+        uint32_t i = 0, src = 0, lo = 0, hi = 0;
+        if (active) {
+            i = A.perm[bin_off + idx];
+            lo = A.off[i];
+            hi = A.off[i + 1];
+            src = A.P[i];
+        }
+        double e_part = 0, s_part = 0;
+        for (uint32_t base = lo + t; base < hi; base += GT * BATCH) {
+            uint32_t jj[BATCH], cc[BATCH];
+            double ww[BATCH];
+#pragma unroll
+            for (int b = 0; b < BATCH; b++) {
+                uint32_t e = base + b * GT;
+                jj[b] = e < hi ? __ldg(A.col + e) : kEmpty;
+                ww[b] = e < hi ? wload<WK>(A.w, e) : 0.0;
+            }
+#pragma unroll
+            for (int b = 0; b < BATCH; b++) cc[b] = jj[b] != kEmpty ? A.P[jj[b]] : kEmpty;
+#pragma unroll
+            for (int b = 0; b < BATCH; b++) {
+                if (jj[b] == kEmpty) continue;
+                const uint32_t c = cc[b];
+                if (c != src) {
+                    if (is_candidate<VER>(c, src, A.up)) {
+                        uint32_t h = table_find_or_insert<SLOTS>(keys, c);
+                        if constexpr (WK == WK_UNIT) atomicAdd(vals + h, 1u);
+                        else atomicAdd(vals + h, ww[b]);
+                    }
+                } else if (jj[b] != i) {
+                    e_part += ww[b];
+                } else {
+                    s_part += ww[b];
+                }
+            }
+        }
+        group_sync<GT>();
+        const double e_src = group_sum<GT>(e_part, red_d);
+        const double selfw = group_sum<GT>(s_part, red_d);
+        double ki = 0, a = 0;
+        if (active) {
+            ki = A.k[i];
+            a = A.sigma[src] - ki;
+        }
+        G best = G(0);
+        uint32_t dst = src;
+#pragma unroll 2
+        for (int s0 = t; s0 < SLOTS; s0 += GT * BATCH) {
+            uint32_t kk[BATCH];
+            double sc[BATCH], kv[BATCH];
+#pragma unroll
+            for (int b = 0; b < BATCH; b++) {
+                int s2 = s0 + b * GT;
+                kk[b] = s2 < SLOTS ? keys[s2] : kEmpty;
+            }
+#pragma unroll
+            for (int b = 0; b < BATCH; b++) {
+                int s2 = s0 + b * GT;
+                if (kk[b] != kEmpty) {
+                    sc[b] = A.sigma[kk[b]];
+                    kv[b] = (double)vals[s2];
+                    keys[s2] = kEmpty;
+                    vals[s2] = V(0);
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < BATCH; b++) {
+                if (kk[b] != kEmpty) {
+                    G gn = Prec<PREC>::gain(kv[b], e_src, ki, a, sc[b], A);
+                    if (better(gn, kk[b], best, dst, A.up)) {
+                        best = gn;
+                        dst = kk[b];
+                    }
+                    dcnt++;
+                }
+            }
+        }
+        group_argmax<GT, G>(best, dst, A.up, red_g, red_c);
+        if (active && t == 0) {
+            A.N[i] = final_choice<VER>(dst, src, A.up);
+            sin += e_src + selfw;
+        }
+        group_sync<GT>();
+    }
+    flush_acc(A.acc, A.integral, sin, dcnt);
+}
+
+// ============================================================================
+// bin 9: global tables, many CTAs per vertex
+// ============================================================================
+constexpr int kHeavyThreads = 256;
+constexpr uint32_t kHeavyChunkE = 4096;  // edges per insert item
+constexpr uint32_t kHeavyChunkS = 4096;  // slots per evaluate item
+
+__device__ __forceinline__ uint32_t find_item(const uint32_t *item_off, uint32_t H, uint32_t q) {
+    // last h with item_off[h] <= q
+    uint32_t lo = 0, hi = H;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (item_off[mid] <= q) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void heavy_layout_kernel(const uint32_t *off, const uint32_t *hv, uint32_t H, uint32_t *tsize,
+                                    uint32_t *ins_cnt, uint32_t *eval_cnt, uint64_t *tsz64) {
+    uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= H) return;
+    uint32_t v = hv[h];
+    uint32_t d = off[v + 1] - off[v];
+    uint32_t ts = (uint32_t)((2ull * d + 63) & ~63ull);
+    tsize[h] = ts;
+    tsz64[h] = ts;
+    ins_cnt[h] = (d + kHeavyChunkE - 1) / kHeavyChunkE;
+    eval_cnt[h] = (ts + kHeavyChunkS - 1) / kHeavyChunkS;
+}
+
+template <int WK, int VER>
+__global__ void __launch_bounds__(kHeavyThreads) heavy_insert_kernel(LMArgs A, const uint32_t *hv, uint32_t H,
+                                                                      const uint32_t *ins_off,
+                                                                      const uint64_t *toff,
+                                                                      const uint32_t *tsize, uint32_t *tkeys,
+                                                                      double *tvals, double *hacc) {
+    constexpr int BATCH = 4;
+    __shared__ double red[2][kHeavyThreads / 32];
+    const uint32_t q = blockIdx.x;
+    const uint32_t h = find_item(ins_off, H, q);
+    const uint32_t v = hv[h];
+    const uint32_t chunk = q - ins_off[h];
+    const uint32_t vlo = A.off[v], vhi = A.off[v + 1];
+    const uint32_t lo = vlo + chunk * kHeavyChunkE;
+    const uint32_t hi = min(vhi, lo + kHeavyChunkE);
+    const uint32_t src = A.P[v];
+    const uint32_t ts = tsize[h];
+    uint32_t *keys = tkeys + toff[h];
+    double *vals = tvals + toff[h];
+    double e_part = 0, s_part = 0;
+    for (uint32_t base = lo + threadIdx.x; base < hi; base += kHeavyThreads * BATCH) {
+        uint32_t jj[BATCH], cc[BATCH];
+        double ww[BATCH];
+#pragma unroll
+        for (int b = 0; b < BATCH; b++) {
+            uint32_t e = base + b * kHeavyThreads;
+            jj[b] = e < hi ? __ldg(A.col + e) : kEmpty;
+            ww[b] = e < hi ? wload<WK>(A.w, e) : 0.0;
+        }
+#pragma unroll
+        for (int b = 0; b < BATCH; b++) cc[b] = jj[b] != kEmpty ? A.P[jj[b]] : kEmpty;
+#pragma unroll
+        for (int b = 0; b < BATCH; b++) {
+            if (jj[b] == kEmpty) continue;
+            const uint32_t c = cc[b];
+            if (c != src) {
+                if (is_candidate<VER>(c, src, A.up)) {
+                    uint32_t s = hash_range(c, ts);
+                    for (uint32_t p = 0; p < ts; p++) {
+                        uint32_t cur = ((volatile uint32_t *)keys)[s];
+                        if (cur == c) break;
+                        if (cur == kEmpty) {
+                            uint32_t prev = atomicCAS(keys + s, kEmpty, c);
+                            if (prev == kEmpty || prev == c) break;
+                        }
+                        s = s + 1 == ts ? 0 : s + 1;
+                    }
+                    atomicAdd(vals + s, ww[b]);
+                }
+            } else if (jj[b] != v) {
+                e_part += ww[b];
+            } else {
+                s_part += ww[b];
+            }
+        }
+    }
+    e_part = warp_sum(e_part);
+    s_part = warp_sum(s_part);
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = e_part;
+        red[1][threadIdx.x >> 5] = s_part;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, b = 0;
+        for (int w2 = 0; w2 < kHeavyThreads / 32; w2++) {
+            a += red[0][w2];
+            b += red[1][w2];
+        }
+        if (a != 0) atomicAdd(hacc + 2 * h, a);
+        if (b != 0) atomicAdd(hacc + 2 * h + 1, b);
+    }
+}
+
+// per evaluate item: packed winner {gain bits, id}
+template <int PREC>
+__global__ void __launch_bounds__(kHeavyThreads) heavy_eval_kernel(LMArgs A, const uint32_t *hv, uint32_t H,
+                                                                    const uint32_t *eval_off,
+                                                                    const uint64_t *toff, const uint32_t *tsize,
+                                                                    uint32_t *tkeys, double *tvals,
+                                                                    const double *hacc,
+                                                                    unsigned long long *item_best) {
+    using G = typename Prec<PREC>::G;
+    __shared__ G rg[32];
+    __shared__ uint32_t rc[32];
+    __shared__ unsigned long long s_d;
+    const uint32_t q = blockIdx.x;
+    const uint32_t h = find_item(eval_off, H, q);
+    const uint32_t v = hv[h];
+    const uint32_t part = q - eval_off[h];
+    const uint32_t ts = tsize[h];
+    const uint32_t lo = part * kHeavyChunkS, hi = min(ts, lo + kHeavyChunkS);
+    uint32_t *keys = tkeys + toff[h];
+    double *vals = tvals + toff[h];
+    const uint32_t src = A.P[v];
+    const double ki = A.k[v];
+    const double a = A.sigma[src] - ki;
+    const double e_src = hacc[2 * h];
+    if (threadIdx.x == 0) s_d = 0;
+    G best = G(0);
+    uint32_t dst = src;
+    unsigned dcnt = 0;
+    for (uint32_t s = lo + threadIdx.x; s < hi; s += kHeavyThreads) {
+        uint32_t c = keys[s];
+        if (c != kEmpty) {
+            double kv = vals[s];
+            keys[s] = kEmpty;
+            vals[s] = 0.0;
+            G gn = Prec<PREC>::gain(kv, e_src, ki, a, A.sigma[c], A);
+            if (better(gn, c, best, dst, A.up)) {
+                best = gn;
+                dst = c;
+            }
+            dcnt++;
+        }
+    }
+    group_argmax<kHeavyThreads, G>(best, dst, A.up, rg, rc);
+    unsigned long long d = warp_sum((unsigned long long)dcnt);
+    if ((threadIdx.x & 31) == 0 && d) atomicAdd(&s_d, d);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long bits;
+        if constexpr (sizeof(G) == 8) bits = *(unsigned long long *)&best;
+        else bits = (unsigned long long)(*(uint32_t *)&best);
+        item_best[2 * q] = bits;
+        item_best[2 * q + 1] = dst;
+        if (s_d) atomicAdd(&A.acc->distinct, s_d);
+    }
+}
+
+template <int PREC, int VER>
+__global__ void heavy_final_kernel(LMArgs A, const uint32_t *hv, uint32_t H, const uint32_t *eval_off,
+                                   double *hacc, const unsigned long long *item_best) {
+    using G = typename Prec<PREC>::G;
+    const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    double sin = 0;
+    if (h < H) {
+        const uint32_t v = hv[h];
+        const uint32_t src = A.P[v];
+        G best = G(0);
+        uint32_t dst = src;
+        for (uint32_t q = eval_off[h]; q < eval_off[h + 1]; q++) {
+            unsigned long long bits = item_best[2 * q];
+            uint32_t c = (uint32_t)item_best[2 * q + 1];
+            G g;
+            if constexpr (sizeof(G) == 8) g = *(G *)&bits;
+            else {
+                uint32_t b32 = (uint32_t)bits;
+                g = *(G *)&b32;
+            }
+            if (better(g, c, best, dst, A.up)) {
+                best = g;
+                dst = c;
+            }
+        }
+        A.N[v] = final_choice<VER>(dst, src, A.up);
+        sin = hacc[2 * h] + hacc[2 * h + 1];
+        hacc[2 * h] = 0;
+        hacc[2 * h + 1] = 0;
+    }
+    flush_acc(A.acc, A.integral, sin, 0);
+}
+
+// ============================================================================
+// sigma / modularity helpers
+// ============================================================================
+__global__ void sigma_update_kernel(const uint32_t *P, const uint32_t *N, const double *k, double *sigma, uint32_t n,
+                                    SweepAcc *acc) {
+    unsigned moved = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        uint32_t a = P[v], b = N[v];
+        if (a != b) {
+            double kv = k[v];
+            atomicAdd(sigma + a, -kv);
+            atomicAdd(sigma + b, kv);
+            moved++;
+        }
+    }
+    unsigned long long m = warp_sum((unsigned long long)moved);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(&acc->moved, m);
+}
+
+__global__ void sigma_sumsq_kernel(const double *sigma, uint32_t n, int integral, SweepAcc *acc) {
+    unsigned long long su = 0;
+    double sf = 0;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        double s = sigma[c];
+        if (integral) {
+            unsigned long long u = (unsigned long long)s;
+            su += u * u;
+        } else {
+            sf += s * s;
+        }
+    }
+    su = warp_sum(su);
+    sf = warp_sum(sf);
+    if ((threadIdx.x & 31) == 0) {
+        if (integral) {
+            if (su) atomicAdd(&acc->s2_u, su);
+        } else if (sf != 0) {
+            atomicAdd(&acc->s2_f, sf);
+        }
+    }
+}
+
+template <int WK>
+__global__ void level_init_kernel(const uint32_t *off, const void *w, uint32_t n, double *k, double *sigma,
+                                  uint32_t *C) {
+    // one warp per vertex
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += (gridDim.x * blockDim.x) >> 5) {
+        uint32_t lo = off[v], hi = off[v + 1];
+        double s;
+        if constexpr (WK == WK_UNIT) {
+            s = (double)(hi - lo);
+        } else {
+            s = 0;
+            for (uint32_t e = lo + lane; e < hi; e += 32) s += wload<WK>(w, e);
+            s = warp_sum(s);
+        }
+        if (lane == 0) {
+            k[v] = s;
+            sigma[v] = s;
+            C[v] = v;
+        }
+    }
+}
+
+template <int WK, int PREC, int VER>
+void launch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, const LMArgs &A, cudaStream_t s) {
+    const Bins &B = lvl.bins;
+    // fork: heavy path on its own stream, the tile and hash bins on others
+    MG_CUDA(cudaEventRecord(ws.ev_fork, s));
+    for (int q = 0; q < 3; q++) MG_CUDA(cudaStreamWaitEvent(ws.streams[q], ws.ev_fork, 0));
+    cudaStream_t sh = ws.streams[0], sm = ws.streams[1], st = ws.streams[2];
+    if (lvl.heavy > 0) {
+        const uint32_t H = lvl.heavy;
+        const uint32_t *hv = ws.perm.get() + B.offset[9];
+        heavy_insert_kernel<WK, VER><<<lvl.ins_items, kHeavyThreads, 0, sh>>>(
+            A, hv, H, ws.h_ins.get(), ws.h_toff.get(), ws.h_tsize.get(), ws.h_keys.get(), ws.h_vals.get(),
+            ws.h_acc.get());
+        MG_LAUNCH_CHECK();
+        heavy_eval_kernel<PREC><<<lvl.eval_items, kHeavyThreads, 0, sh>>>(
+            A, hv, H, ws.h_eval.get(), ws.h_toff.get(), ws.h_tsize.get(), ws.h_keys.get(), ws.h_vals.get(),
+            ws.h_acc.get(), ws.h_best.get());
+        MG_LAUNCH_CHECK();
+        heavy_final_kernel<PREC, VER><<<(unsigned)ceil_div(H, 256), 256, 0, sh>>>(A, hv, H, ws.h_eval.get(),
+                                                                                  ws.h_acc.get(), ws.h_best.get());
+        MG_LAUNCH_CHECK();
+    }
+    using V = typename ValT<WK>::type;
+    auto hash_launch = [&](auto kern, int slots, int gpb, int block, int bin, cudaStream_t str) {
+        if (B.size[bin] == 0) return;
+        size_t smem = (size_t)slots * gpb * (sizeof(uint32_t) + sizeof(V));
+        MG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(B.size[bin], gpb), 148ull * 64);
+        kern<<<grid, block, smem, str>>>(A, B.offset[bin], B.size[bin]);
+        MG_LAUNCH_CHECK();
+    };
+    hash_launch(lm_hash_kernel<512, 8192, WK, PREC, VER, 512>, 8192, 1, 512, 8, sm);
+    hash_launch(lm_hash_kernel<256, 4096, WK, PREC, VER, 256>, 4096, 1, 256, 7, sm);
+    hash_launch(lm_hash_kernel<128, 1024, WK, PREC, VER, 128>, 1024, 1, 128, 6, sm);
+    hash_launch(lm_hash_kernel<32, 256, WK, PREC, VER, 256>, 256, 8, 256, 5, st);
+    auto tile_launch = [&](auto kern, int T, int bin, cudaStream_t str) {
+        if (B.size[bin] == 0) return;
+        uint64_t groups_per_block = 256 / T;
+        unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(B.size[bin], groups_per_block), 148ull * 32);
+        kern<<<grid, 256, 0, str>>>(A, B.offset[bin], B.size[bin]);
+        MG_LAUNCH_CHECK();
+    };
+    tile_launch(lm_tile_kernel<32, WK, PREC, VER>, 32, 4, st);
+    tile_launch(lm_tile_kernel<16, WK, PREC, VER>, 16, 3, st);
+    tile_launch(lm_tile_kernel<8, WK, PREC, VER>, 8, 2, st);
+    tile_launch(lm_tile_kernel<4, WK, PREC, VER>, 4, 1, st);
+    tile_launch(lm_tile_kernel<2, WK, PREC, VER>, 2, 0, st);
+    for (int q = 0; q < 3; q++) {
+        MG_CUDA(cudaEventRecord(ws.ev_join[q], ws.streams[q]));
+        MG_CUDA(cudaStreamWaitEvent(s, ws.ev_join[q], 0));
+    }
+}
+
+}  // namespace
+
+MoveWorkspace::~MoveWorkspace() {
+    for (auto &s : streams)
+        if (s) cudaStreamDestroy(s);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    for (auto &e : ev_join)
+        if (e) cudaEventDestroy(e);
+}
+
+void MoveWorkspace::init_streams() {
+    if (streams[0]) return;
+    for (auto &s : streams) MG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    MG_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    for (auto &e : ev_join) MG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+}
+
+void move_prepare_level(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, cudaStream_t s) {
+    ws.init_streams();
+    ws.acc.ensure(1);
+    uint32_t *perm = ws.perm.ensure(g.n + 1);
+    compute_bins(0, g.n, g.off, perm, lvl.bins, s, ws.prim);
+    lvl.heavy = lvl.bins.size[9];
+    lvl.ins_items = lvl.eval_items = 0;
+    lvl.table_slots = 0;
+    if (lvl.heavy == 0) return;
+    const uint32_t H = lvl.heavy;
+    const uint32_t *hv = perm + lvl.bins.offset[9];
+    uint32_t *tsize = ws.h_tsize.ensure(H + 1);
+    uint32_t *ins = ws.h_ins.ensure(H + 1);
+    uint32_t *ev = ws.h_eval.ensure(H + 1);
+    uint64_t *toff = ws.h_toff.ensure(H + 1);
+    uint64_t *tmp = ws.tmp64.ensure(H + 1);
+    heavy_layout_kernel<<<(unsigned)ceil_div(H, 256), 256, 0, s>>>(g.off, hv, H, tsize, ins, ev, tmp);
+    MG_LAUNCH_CHECK();
+    exclusive_scan<uint32_t>(ins, ins, H, ins + H, s, ws.prim);
+    exclusive_scan<uint32_t>(ev, ev, H, ev + H, s, ws.prim);
+    exclusive_scan<uint64_t>(tmp, toff, H, toff + H, s, ws.prim);
+    uint32_t ni = 0, ne = 0;
+    uint64_t slots = 0;
+    MG_CUDA(cudaMemcpyAsync(&ni, ins + H, sizeof ni, cudaMemcpyDeviceToHost, s));
+    MG_CUDA(cudaMemcpyAsync(&ne, ev + H, sizeof ne, cudaMemcpyDeviceToHost, s));
+    MG_CUDA(cudaMemcpyAsync(&slots, toff + H, sizeof slots, cudaMemcpyDeviceToHost, s));
+    MG_CUDA(cudaStreamSynchronize(s));
+    lvl.ins_items = ni;
+    lvl.eval_items = ne;
+    lvl.table_slots = slots;
+    uint32_t *keys = ws.h_keys.ensure(slots);
+    double *vals = ws.h_vals.ensure(slots);
+    MG_CUDA(cudaMemsetAsync(keys, 0xFF, slots * sizeof(uint32_t), s));
+    MG_CUDA(cudaMemsetAsync(vals, 0, slots * sizeof(double), s));
+    double *hacc = ws.h_acc.ensure(2ull * H);
+    MG_CUDA(cudaMemsetAsync(hacc, 0, 2ull * H * sizeof(double), s));
+    ws.h_best.ensure(2ull * ne + 2);
+}
+
+void sweep_reset_acc(MoveWorkspace &ws, cudaStream_t s) {
+    MG_CUDA(cudaMemsetAsync(ws.acc.ensure(1), 0, sizeof(SweepAcc), s));
+}
+
+void move_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p,
+                const uint32_t *P, uint32_t *N, const double *k, const double *sigma, cudaStream_t s) {
+    LMArgs A;
+    A.off = g.off;
+    A.col = g.col;
+    A.w = g.w;
+    A.P = P;
+    A.N = N;
+    A.k = k;
+    A.sigma = sigma;
+    A.perm = ws.perm.get();
+    A.m = p.mass / 2.0;
+    A.m_f = (float)(p.mass / 2.0);
+    A.mass_i = (long long)p.mass;
+    A.up = p.up;
+    A.integral = p.integral;
+    A.acc = ws.acc.ensure(1);
+    MG_CHECK(p.version == 1 || p.version == 2, MG_ERR_INVALID, "version must be 0, 1 or 2");
+    if (p.precision == MG_PREC_INT64)
+        MG_CHECK(p.integral && p.mass < 2147483648.0, MG_ERR_UNSUPPORTED,
+                 "int64 precision needs integral weights with total below 2^31");
+#define MG_SWEEP_CASE(WKV, PRECV)                                                                  \
+    if (g.wk == WKV && p.precision == PRECV) {                                                     \
+        if (p.version == 1) launch_sweep<WKV, PRECV, 1>(g, lvl, ws, A, s);                         \
+        else launch_sweep<WKV, PRECV, 2>(g, lvl, ws, A, s);                                        \
+        return;                                                                                    \
+    }
+    MG_SWEEP_CASE(WK_UNIT, MG_PREC_FP64)
+    MG_SWEEP_CASE(WK_F32, MG_PREC_FP64)
+    MG_SWEEP_CASE(WK_F64, MG_PREC_FP64)
+    MG_SWEEP_CASE(WK_UNIT, MG_PREC_INT64)
+    MG_SWEEP_CASE(WK_F32, MG_PREC_INT64)
+    MG_SWEEP_CASE(WK_F64, MG_PREC_INT64)
+    MG_SWEEP_CASE(WK_UNIT, MG_PREC_FP32)
+    MG_SWEEP_CASE(WK_F32, MG_PREC_FP32)
+    MG_SWEEP_CASE(WK_F64, MG_PREC_FP32)
+#undef MG_SWEEP_CASE
+    throw Error(MG_ERR_INVALID, "unknown weight kind or precision");
+}
+
+void sigma_sumsq(const double *sigma, uint32_t n, int integral, MoveWorkspace &ws, cudaStream_t s) {
+    if (n == 0) return;
+    unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(n, 256), 148ull * 8);
+    sigma_sumsq_kernel<<<grid, 256, 0, s>>>(sigma, n, integral, ws.acc.ensure(1));
+    MG_LAUNCH_CHECK();
+}
+
+void sigma_update(const uint32_t *P, const uint32_t *N, const double *k, double *sigma, uint32_t n,
+                  MoveWorkspace &ws, cudaStream_t s) {
+    if (n == 0) return;
+    unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(n, 256), 148ull * 8);
+    sigma_update_kernel<<<grid, 256, 0, s>>>(P, N, k, sigma, n, ws.acc.ensure(1));
+    MG_LAUNCH_CHECK();
+}
+
+void level_init(const GraphView &g, double *k, double *sigma, uint32_t *C, cudaStream_t s) {
+    if (g.n == 0) return;
+    unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(g.n, 8), 148ull * 16);
+    if (g.wk == WK_UNIT) level_init_kernel<WK_UNIT><<<grid, 256, 0, s>>>(g.off, g.w, g.n, k, sigma, C);
+    else if (g.wk == WK_F32) level_init_kernel<WK_F32><<<grid, 256, 0, s>>>(g.off, g.w, g.n, k, sigma, C);
+    else level_init_kernel<WK_F64><<<grid, 256, 0, s>>>(g.off, g.w, g.n, k, sigma, C);
+    MG_LAUNCH_CHECK();
+}
+
+double modularity_from_acc(const SweepAcc &a, double mass, int integral) {
+    if (integral) return (double)a.sin_u / mass - (double)a.s2_u / (mass * mass);
+    return a.sin_f / mass - a.s2_f / (mass * mass);
+}
+
+}  // namespace mg
