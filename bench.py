@@ -227,7 +227,7 @@ def run_engine(args, world, rank, local, pg):
     last = runs[-1]
     sweep_s = sum(r["seconds_sweep_kernels"] for r in runs)
     sweep_b = sum(r["sweep_bytes"] for r in runs)
-    sweeps = sum(r["iterations"] for r in runs)
+    sweeps = sum(r["sweeps"] for r in runs)
     achieved = sweep_b / sweep_s / 1e9
     peak, peak_kind = peaks()
     traffic = traffic_per_sweep()
@@ -236,7 +236,7 @@ def run_engine(args, world, rank, local, pg):
     # run, read the assignment back
     off, cols, _ = g.csr()
     e2e_t, e2e_e = 0.0, 0
-    for i in range(args.e2e_steps + 1):
+    for i in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
         t0 = time.perf_counter()
         h = ctx.graph_from_csr(info["n"], off, cols, None)
         r = h.louvain()
@@ -283,7 +283,7 @@ def run_engine(args, world, rank, local, pg):
                      "kernel": "local-move sweep (all bins)", "peak_kind": peak_kind,
                      "sweeps": sweeps, "algorithmic_bytes_per_sweep": sweep_b / max(sweeps, 1)},
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_esum / e2e_tmax if e2e_tmax > 0 else None, "unit": UNIT,
+        "e2e": None if args.e2e_steps <= 0 else {"value": e2e_esum / e2e_tmax, "unit": UNIT,
                 "h2d_bytes_per_step": 8 * (info["n"] + 1) + 4 * info["nnz"],
                 "d2h_bytes_per_step": 4 * info["n"]},
         "clocks": clk,

@@ -146,7 +146,7 @@ typedef struct {
     double modularity;       /* final Q */
     int phases;              /* coarsening steps taken */
     int levels;              /* phases started */
-    int iterations;          /* local-move sweeps */
+    int iterations;          /* local-move iterations as the reference counts them */
     uint32_t communities;    /* final community count */
     double seconds_total;    /* device time of the whole run */
     double seconds_local_move;
@@ -158,6 +158,7 @@ typedef struct {
     double seconds_sweep_kernels; /* device time of the local-move kernels alone */
     double sweep_bytes;      /* algorithmic bytes of those sweeps: 12E + 24V + 8D each */
     uint64_t kernel_launches; /* engine kernels launched during the run */
+    uint64_t sweeps;         /* edge passes run (iterations + one per phase) */
 } mg_summary;
 
 /* Run Louvain to convergence.  Replaces louvain::run / louvain_gl::run /

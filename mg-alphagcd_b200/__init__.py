@@ -58,7 +58,7 @@ class _Summary(ct.Structure):
                 ("edges_swept", ct.c_uint64), ("phase0_edges_swept", ct.c_uint64),
                 ("phase0_seconds", ct.c_double), ("distinct_pairs", ct.c_uint64),
                 ("seconds_sweep_kernels", ct.c_double), ("sweep_bytes", ct.c_double),
-                ("kernel_launches", ct.c_uint64)]
+                ("kernel_launches", ct.c_uint64), ("sweeps", ct.c_uint64)]
 
 
 EXPORTED = [

@@ -29,16 +29,40 @@ __global__ void apply_relabel_kernel(const uint32_t *C, uint32_t n, const uint32
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) Cd[v] = newid[C[v]];
 }
 
-// one warp per row: key = (C'[u] << bc) | C'[v], payload = weight (if any)
+// key = (C'[u] << bc) | C'[v] per edge (u,v), payload = weight (if any).
+// Edge-parallel: a warp takes 512 consecutive edges (lane-strided, coalesced),
+// finds the row of the first by binary search and walks rows forward.
 template <int WK>
-__global__ void expand_keys_kernel(const uint32_t *off, const uint32_t *col, const void *w, uint32_t n,
+__global__ void expand_keys_kernel(const uint32_t *off, const uint32_t *col, const void *w, uint32_t n, uint64_t m,
                                    const uint32_t *Cd, int bc, uint64_t *keys, double *vals) {
+    constexpr int PER = 16;
     const uint32_t lane = threadIdx.x & 31;
-    for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < n; u += (gridDim.x * blockDim.x) >> 5) {
-        const uint32_t lo = off[u], hi = off[u + 1];
-        const uint64_t r = (uint64_t)Cd[u] << bc;
-        for (uint32_t e = lo + lane; e < hi; e += 32) {
-            keys[e] = r | Cd[col[e]];
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t t0 = warp * 32 * PER; t0 < m; t0 += nw * 32 * PER) {
+        uint32_t r = 0;
+        if (lane == 0) {
+            uint32_t lo = 0, hi = n - 1;  // last row with off[row] <= t0
+            while (lo < hi) {
+                uint32_t mid = lo + ((hi - lo + 1) >> 1);
+                if (off[mid] <= t0) lo = mid;
+                else hi = mid - 1;
+            }
+            r = lo;
+        }
+        r = __shfl_sync(0xffffffffu, r, 0);
+        uint32_t cr = kEmpty;
+        uint64_t kr = 0;
+#pragma unroll 4
+        for (int k = 0; k < PER; k++) {
+            const uint64_t e = t0 + (uint64_t)k * 32 + lane;
+            if (e >= m) break;
+            while (off[r + 1] <= e) r++;
+            if (r != cr) {
+                cr = r;
+                kr = (uint64_t)Cd[r] << bc;
+            }
+            keys[e] = kr | Cd[__ldcs(col + e)];
             if constexpr (WK == WK_F32) vals[e] = (double)((const float *)w)[e];
             else if constexpr (WK == WK_F64) vals[e] = ((const double *)w)[e];
         }
@@ -238,10 +262,11 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
     const bool weighted = g.wk != WK_UNIT;
     double *vals = weighted ? ws.vals.ensure(m + 1) : nullptr;
     double *vals2 = weighted ? ws.vals_alt.ensure(m + 1) : nullptr;
-    unsigned gw = grid_for((uint64_t)g.n * 32);
-    if (g.wk == WK_UNIT) expand_keys_kernel<WK_UNIT><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, Cd, bc, keys, vals);
-    else if (g.wk == WK_F32) expand_keys_kernel<WK_F32><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, Cd, bc, keys, vals);
-    else expand_keys_kernel<WK_F64><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, Cd, bc, keys, vals);
+    unsigned gw = grid_for(ceil_div(m, 16), 256, 148ull * 64);
+    if (g.wk == WK_UNIT) expand_keys_kernel<WK_UNIT><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, vals);
+    else if (g.wk == WK_F32)
+        expand_keys_kernel<WK_F32><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, vals);
+    else expand_keys_kernel<WK_F64><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, vals);
     MG_LAUNCH_CHECK();
     bool flipped;
     if (weighted) flipped = radix_sort<double>(keys, vals, keys2, vals2, m, 2 * bc, s, ws.prim);

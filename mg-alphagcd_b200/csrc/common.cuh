@@ -45,6 +45,12 @@ constexpr uint32_t kEmpty = 0xFFFFFFFFu;
 constexpr int kNumSMs = 148;
 
 enum WeightKind { WK_UNIT = 0, WK_F32 = 1, WK_F64 = 2 };
+// Kernel variants: weights stored as f32 / f64 whose values are integral
+// (every coarsened level of an integral graph) accumulate in 32-bit integer
+// table slots, which shared and distributed shared memory add natively.
+enum { WK_F32I = 3, WK_F64I = 4 };
+template <int WK>
+constexpr bool kIntg = WK == WK_UNIT || WK == WK_F32I || WK == WK_F64I;
 
 inline uint64_t ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
 inline uint32_t pow2_at_least(uint64_t x, uint32_t lo = 16) {
@@ -88,6 +94,30 @@ __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
+}
+
+// Correctly rounded x / d for a divisor fixed for the whole run, with its
+// reciprocal r = RN(1/d) computed once on the host: q0 = RN(x*r) lies within
+// one ulp of x/d, the remainder x - q0*d is exact in one fma, and
+// RN(q0 + rem*r) is then the correctly rounded quotient (Markstein's
+// theorem; J.-M. Muller et al., Handbook of Floating-Point Arithmetic,
+// ch. 5).  No intermediate of the gain overflows or underflows.  It keeps the
+// arithmetic on the FP64 pipe instead of the special-function unit that a
+// divide instruction sequence uses.
+__device__ __forceinline__ double div_by(double x, double d, double r) {
+    const double q0 = __dmul_rn(x, r);
+    const double rem = __fma_rn(-q0, d, x);
+    return __fma_rn(rem, r, q0);
+}
+__device__ __forceinline__ float div_by(float x, float d, float r) {
+    const float q0 = __fmul_rn(x, r);
+    const float rem = __fmaf_rn(-q0, d, x);
+    return __fmaf_rn(rem, r, q0);
+}
+// exact uint32 -> double with one FP64 subtraction: the bits 0x43300000:x
+// encode 2^52 + x
+__device__ __forceinline__ double u2d(uint32_t x) {
+    return __dsub_rn(__hiloint2double(0x43300000, (int)x), 4503599627370496.0);
 }
 
 // Multiplicative hash onto [0, 2^bits)

@@ -46,10 +46,19 @@ struct SweepAcc {
     double pad[2];
 };
 
+// Heavy vertices (last bin) are split into tiers by degree: tier t < 5 is
+// served by clusters of 2^t CTAs holding one distributed shared-memory table
+// of 2^t * kClusterSlots slots (load <= 1/2); the last tier (giants) by the
+// multi-CTA global-table path.
+constexpr int kClusterSlots = 16384;
+constexpr int kTiers = 6;
+
 // Per-level state of the local-move engine: bins and the heavy-vertex tables.
 struct MoveLevel {
     Bins bins;
     uint32_t heavy = 0;            // vertices in the last bin
+    uint32_t tier_off[kTiers + 1] = {0};  // heavy vertices by tier (ws.h_tier)
+    uint32_t giants = 0;           // vertices on the global-table path
     uint32_t ins_items = 0;        // insert work items (vertex, edge chunk)
     uint32_t eval_items = 0;       // evaluate work items (vertex, slot chunk)
     uint64_t table_slots = 0;
@@ -57,6 +66,9 @@ struct MoveLevel {
 
 struct MoveWorkspace {
     DBuf<uint32_t> perm;
+    DBuf<uint32_t> h_tier;         // heavy vertices grouped by tier
+    DBuf<uint32_t> h_deg;          // degrees of the heavy vertices
+    int max_cluster = 0;           // largest cluster size the device runs (8 or 16)
     // heavy-vertex global tables
     DBuf<uint64_t> h_toff;         // table offset per heavy vertex (H+1)
     DBuf<uint32_t> h_tsize;        // table size per heavy vertex

@@ -28,7 +28,10 @@
 // community of P (self-loops included), the first term of the modularity of P
 // (src/louvain/louvain.cu:105-238), so a separate modularity pass over the
 // edges is not needed.
+#include <cooperative_groups.h>
+
 #include <algorithm>
+#include <vector>
 
 #include "engine.cuh"
 
@@ -46,7 +49,9 @@ struct LMArgs {
     const double *__restrict__ sigma;
     const uint32_t *__restrict__ perm;
     double m;            // mass / 2
-    float m_f;
+    double two_m;        // mass
+    double r_m, r_two_m; // RN(1/m), RN(1/(2m))
+    float m_f, two_m_f, r_m_f, r_two_m_f;
     long long mass_i;    // mass (integral graphs)
     int up;
     int integral;
@@ -56,8 +61,8 @@ struct LMArgs {
 template <int WK>
 __device__ __forceinline__ double wload(const void *w, uint32_t e) {
     if constexpr (WK == WK_UNIT) return 1.0;
-    else if constexpr (WK == WK_F32) return (double)__ldg((const float *)w + e);
-    else return __ldg((const double *)w + e);
+    else if constexpr (WK == WK_F32 || WK == WK_F32I) return (double)__ldcs((const float *)w + e);
+    else return __ldcs((const double *)w + e);
 }
 
 // ---- gain in the three precision modes -------------------------------------
@@ -66,13 +71,15 @@ struct Prec;
 template <>
 struct Prec<MG_PREC_FP64> {
     using G = double;
-    // (k_ic - (e - k_i*(a - s_c)/(2m))) / m, each operation rounded as written
+    // (k_ic - (e - k_i*(a - s_c)/(2m))) / m, each operation rounded as written;
+    // both quotients are correctly rounded (div_by), so the value is the one a
+    // divide instruction gives
     __device__ static __forceinline__ G gain(double kic, double e, double ki, double a, double sc,
                                              const LMArgs &A) {
         double t = __dmul_rn(ki, __dsub_rn(a, sc));
-        t = __ddiv_rn(t, __dmul_rn(2.0, A.m));
+        t = div_by(t, A.two_m, A.r_two_m);
         t = __dsub_rn(e, t);
-        return __ddiv_rn(__dsub_rn(kic, t), A.m);
+        return div_by(__dsub_rn(kic, t), A.m, A.r_m);
     }
 };
 template <>
@@ -81,9 +88,9 @@ struct Prec<MG_PREC_FP32> {
     __device__ static __forceinline__ G gain(double kic, double e, double ki, double a, double sc,
                                              const LMArgs &A) {
         float t = __fmul_rn((float)ki, __fsub_rn((float)a, (float)sc));
-        t = __fdiv_rn(t, __fmul_rn(2.0f, A.m_f));
+        t = div_by(t, A.two_m_f, A.r_two_m_f);
         t = __fsub_rn((float)e, t);
-        return __fdiv_rn(__fsub_rn((float)kic, t), A.m_f);
+        return div_by(__fsub_rn((float)kic, t), A.m_f, A.r_m_f);
     }
 };
 template <>
@@ -175,7 +182,7 @@ __global__ void __launch_bounds__(256) lm_tile_kernel(LMArgs A, uint32_t bin_off
         uint32_t j = kEmpty, c = kEmpty;
         double w = 0;
         if (has) {
-            j = __ldg(A.col + e);
+            j = __ldcs(A.col + e);
             w = wload<WK>(A.w, e);
             c = A.P[j];
         }
@@ -191,9 +198,9 @@ __global__ void __launch_bounds__(256) lm_tile_kernel(LMArgs A, uint32_t bin_off
         const bool leader = cand && (uint32_t)(__ffs(peers) - 1) == lane;
         double kic, e_src, selfw;
         if constexpr (WK == WK_UNIT) {
-            kic = (double)__popc(peers);
-            e_src = (double)__popc(__ballot_sync(0xffffffffu, inner) & gmask);
-            selfw = (double)__popc(__ballot_sync(0xffffffffu, self) & gmask);
+            kic = u2d(__popc(peers));
+            e_src = u2d(__popc(__ballot_sync(0xffffffffu, inner) & gmask));
+            selfw = u2d(__popc(__ballot_sync(0xffffffffu, self) & gmask));
         } else {
             wbuf[warp][lane] = w;
             __syncwarp();
@@ -245,13 +252,10 @@ __global__ void __launch_bounds__(256) lm_tile_kernel(LMArgs A, uint32_t bin_off
 // ============================================================================
 // bins 5-8: GT threads per vertex, SLOTS-entry shared table
 // ============================================================================
+// table value type: 32-bit integer sums for integral weights, else double
 template <int WK>
 struct ValT {
-    using type = double;
-};
-template <>
-struct ValT<WK_UNIT> {
-    using type = uint32_t;
+    using type = typename std::conditional<kIntg<WK>, uint32_t, double>::type;
 };
 
 template <int GT>
@@ -317,8 +321,8 @@ struct Log2<1> {
 };
 
 template <int SLOTS>
-__device__ __forceinline__ uint32_t table_find_or_insert(uint32_t *keys, uint32_t c) {
-    constexpr int bits = Log2<SLOTS>::value;
+__device__ __forceinline__ uint32_t table_find_or_insert(uint32_t *keys, uint32_t c, int bits) {
+    const uint32_t mask = (1u << bits) - 1u;
     uint32_t h = hash_slot(c, bits);
     for (int p = 0; p < SLOTS; p++) {
         uint32_t cur = ((volatile uint32_t *)keys)[h];
@@ -327,13 +331,21 @@ __device__ __forceinline__ uint32_t table_find_or_insert(uint32_t *keys, uint32_
             uint32_t prev = atomicCAS(keys + h, kEmpty, c);
             if (prev == kEmpty || prev == c) return h;
         }
-        h = (h + 1) & (SLOTS - 1);
+        h = (h + 1) & mask;
     }
     return kEmpty;  // unreachable: tables hold >= 2*deg slots
 }
 
+// table bits for a vertex of degree d: 2*d slots rounded up to a power of
+// two, at least 32, at most the group's table
+template <int SLOTS>
+__device__ __forceinline__ int table_bits(uint32_t d) {
+    const int want = d <= 16 ? 5 : 33 - __clz(2 * d - 1);
+    return want < Log2<SLOTS>::value ? want : Log2<SLOTS>::value;
+}
+
 template <int GT, int SLOTS, int WK, int PREC, int VER, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) lm_hash_kernel(LMArgs A, uint32_t bin_off, uint32_t bin_size) {
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) lm_hash_kernel(LMArgs A, uint32_t bin_off, uint32_t bin_size) {
     using G = typename Prec<PREC>::G;
     using V = typename ValT<WK>::type;
     constexpr int GPB = BLOCK / GT;
@@ -358,12 +370,17 @@ __global__ void __launch_bounds__(BLOCK) lm_hash_kernel(LMArgs A, uint32_t bin_o
         // the loop condition is uniform inside a group (GT == 32) or block (GT > 32)
         const bool active = idx < bin_size;
         uint32_t i = 0, src = 0, lo = 0, hi = 0;
+        double ki = 0, a = 0;
         if (active) {
             i = A.perm[bin_off + idx];
             lo = A.off[i];
             hi = A.off[i + 1];
             src = A.P[i];
+            ki = A.k[i];
+            a = A.sigma[src] - ki;  // issued early, consumed after the edge pass
         }
+        const int tb = table_bits<SLOTS>(hi - lo);
+        const int tsz = 1 << tb;
         double e_part = 0, s_part = 0;
         for (uint32_t base = lo + t; base < hi; base += GT * BATCH) {
             uint32_t jj[BATCH], cc[BATCH];
@@ -371,7 +388,7 @@ __global__ void __launch_bounds__(BLOCK) lm_hash_kernel(LMArgs A, uint32_t bin_o
 #pragma unroll
             for (int b = 0; b < BATCH; b++) {
                 uint32_t e = base + b * GT;
-                jj[b] = e < hi ? __ldg(A.col + e) : kEmpty;
+                jj[b] = e < hi ? __ldcs(A.col + e) : kEmpty;
                 ww[b] = e < hi ? wload<WK>(A.w, e) : 0.0;
             }
 #pragma unroll
@@ -382,8 +399,8 @@ __global__ void __launch_bounds__(BLOCK) lm_hash_kernel(LMArgs A, uint32_t bin_o
                 const uint32_t c = cc[b];
                 if (c != src) {
                     if (is_candidate<VER>(c, src, A.up)) {
-                        uint32_t h = table_find_or_insert<SLOTS>(keys, c);
-                        if constexpr (WK == WK_UNIT) atomicAdd(vals + h, 1u);
+                        uint32_t h = table_find_or_insert<SLOTS>(keys, c, tb);
+                        if constexpr (kIntg<WK>) atomicAdd(vals + h, (uint32_t)ww[b]);
                         else atomicAdd(vals + h, ww[b]);
                     }
                 } else if (jj[b] != i) {
@@ -396,34 +413,31 @@ __global__ void __launch_bounds__(BLOCK) lm_hash_kernel(LMArgs A, uint32_t bin_o
         group_sync<GT>();
         const double e_src = group_sum<GT>(e_part, red_d);
         const double selfw = group_sum<GT>(s_part, red_d);
-        double ki = 0, a = 0;
-        if (active) {
-            ki = A.k[i];
-            a = A.sigma[src] - ki;
-        }
         G best = G(0);
         uint32_t dst = src;
-#pragma unroll 2
-        for (int s0 = t; s0 < SLOTS; s0 += GT * BATCH) {
-            uint32_t kk[BATCH];
-            double sc[BATCH], kv[BATCH];
+        // every slot of this thread in one batch, so the sigma gathers overlap
+        constexpr int EB = SLOTS / GT < 8 ? SLOTS / GT : 8;
+        for (int s0 = t; s0 < tsz; s0 += GT * EB) {
+            uint32_t kk[EB];
+            double sc[EB], kv[EB];
 #pragma unroll
-            for (int b = 0; b < BATCH; b++) {
+            for (int b = 0; b < EB; b++) {
                 int s2 = s0 + b * GT;
-                kk[b] = s2 < SLOTS ? keys[s2] : kEmpty;
+                kk[b] = s2 < tsz ? keys[s2] : kEmpty;
             }
 #pragma unroll
-            for (int b = 0; b < BATCH; b++) {
+            for (int b = 0; b < EB; b++) {
                 int s2 = s0 + b * GT;
                 if (kk[b] != kEmpty) {
                     sc[b] = A.sigma[kk[b]];
-                    kv[b] = (double)vals[s2];
+                    if constexpr (kIntg<WK>) kv[b] = u2d(vals[s2]);
+                    else kv[b] = (double)vals[s2];
                     keys[s2] = kEmpty;
                     vals[s2] = V(0);
                 }
             }
 #pragma unroll
-            for (int b = 0; b < BATCH; b++) {
+            for (int b = 0; b < EB; b++) {
                 if (kk[b] != kEmpty) {
                     G gn = Prec<PREC>::gain(kv[b], e_src, ki, a, sc[b], A);
                     if (better(gn, kk[b], best, dst, A.up)) {
@@ -445,7 +459,208 @@ __global__ void __launch_bounds__(BLOCK) lm_hash_kernel(LMArgs A, uint32_t bin_o
 }
 
 // ============================================================================
-// bin 9: global tables, many CTAs per vertex
+// bin 9, tiers 0-4: one vertex per thread-block cluster of CS CTAs, the
+// cluster's distributed shared memory holding one hash table of CS *
+// kClusterSlots slots.  A neighbour community hashes to (owner CTA, slot);
+// inserts into other CTAs' segments go through DSMEM atomics; each CTA then
+// evaluates the candidates of its own segment, and rank 0 reduces the CS
+// winners.  Two cluster barriers per vertex (accumulators double-buffered).
+// Unit weights use packed 64-bit slots {key:32 | count:32}.
+// ============================================================================
+namespace cg = cooperative_groups;
+constexpr int kClusterThreads = 1024;
+constexpr uint64_t kEmpty64 = 0xFFFFFFFF00000000ull;
+
+template <int CS>
+__device__ __forceinline__ void cluster_barrier() {
+    if constexpr (CS == 1) __syncthreads();
+    else cg::this_cluster().sync();
+}
+
+template <int CS, class T>
+__device__ __forceinline__ T *rank_ptr(T *p, unsigned r) {
+    if constexpr (CS == 1) return p;
+    else return cg::this_cluster().map_shared_rank(p, r);
+}
+
+template <int CS, int WK, int PREC, int VER>
+__global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A, const uint32_t *verts,
+                                                                        uint32_t count) {
+    using G = typename Prec<PREC>::G;
+    constexpr int S = kClusterSlots;
+    constexpr int BATCH = 4;
+    constexpr int EB = 4;  // slots per thread per evaluation batch
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint64_t *packed = (uint64_t *)smem_raw;                 // integral weights
+    uint32_t *keys = (uint32_t *)smem_raw;                   // real weights
+    double *vals = (double *)(smem_raw + sizeof(uint32_t) * S);
+    __shared__ double acc_e[2], acc_s[2];
+    __shared__ G best_g[2][CS];
+    __shared__ uint32_t best_c[2][CS];
+    __shared__ G red_g[32];
+    __shared__ uint32_t red_c[32];
+    unsigned rank = 0;
+    if constexpr (CS > 1) rank = cg::this_cluster().block_rank();
+    for (int s = threadIdx.x; s < S; s += kClusterThreads) {
+        if constexpr (kIntg<WK>) packed[s] = kEmpty64;
+        else {
+            keys[s] = kEmpty;
+            vals[s] = 0.0;
+        }
+    }
+    if (threadIdx.x < 2) {
+        acc_e[threadIdx.x] = 0;
+        acc_s[threadIdx.x] = 0;
+    }
+    cluster_barrier<CS>();
+    const uint32_t cluster_id = blockIdx.x / CS, nclusters = gridDim.x / CS;
+    const uint32_t tc = rank * kClusterThreads + threadIdx.x;
+    constexpr uint32_t stride = CS * kClusterThreads;
+    double sin = 0;
+    unsigned dcnt = 0;
+    int par = 0;
+    for (uint32_t vi = cluster_id; vi < count; vi += nclusters, par ^= 1) {
+        const uint32_t i = verts[vi];
+        const uint32_t lo = A.off[i], hi = A.off[i + 1], src = A.P[i];
+        const double ki = A.k[i];
+        const double a = A.sigma[src] - ki;
+        double e_part = 0, s_part = 0;
+        for (uint32_t base = lo + tc; base < hi; base += stride * BATCH) {
+            uint32_t jj[BATCH], cc[BATCH];
+            double ww[BATCH];
+#pragma unroll
+            for (int b = 0; b < BATCH; b++) {
+                uint32_t e = base + b * stride;
+                jj[b] = e < hi ? __ldcs(A.col + e) : kEmpty;
+                ww[b] = e < hi ? wload<WK>(A.w, e) : 0.0;
+            }
+#pragma unroll
+            for (int b = 0; b < BATCH; b++) cc[b] = jj[b] != kEmpty ? A.P[jj[b]] : kEmpty;
+#pragma unroll
+            for (int b = 0; b < BATCH; b++) {
+                if (jj[b] == kEmpty) continue;
+                const uint32_t c = cc[b];
+                if (c != src) {
+                    if (!is_candidate<VER>(c, src, A.up)) continue;
+                    const uint32_t h = hash_range(c, (uint32_t)CS * S);
+                    const unsigned owner = h / S;
+                    uint32_t s = h & (S - 1);
+                    if constexpr (kIntg<WK>) {
+                        const unsigned long long wi = (uint32_t)ww[b];
+                        uint64_t *seg = rank_ptr<CS>(packed, owner);
+                        for (int p = 0; p < S; p++) {
+                            uint64_t cur = ((volatile uint64_t *)seg)[s];
+                            uint32_t k = (uint32_t)(cur >> 32);
+                            if (k == c) {
+                                atomicAdd((unsigned long long *)(seg + s), wi);
+                                break;
+                            }
+                            if (k == kEmpty) {
+                                uint64_t prev = atomicCAS((unsigned long long *)(seg + s), kEmpty64,
+                                                          ((uint64_t)c << 32) | wi);
+                                if (prev == kEmpty64) break;
+                                if ((uint32_t)(prev >> 32) == c) {
+                                    atomicAdd((unsigned long long *)(seg + s), wi);
+                                    break;
+                                }
+                            }
+                            s = (s + 1) & (S - 1);
+                        }
+                    } else {
+                        uint32_t *ks = rank_ptr<CS>(keys, owner);
+                        double *vs = rank_ptr<CS>(vals, owner);
+                        for (int p = 0; p < S; p++) {
+                            uint32_t cur = ((volatile uint32_t *)ks)[s];
+                            if (cur == c) break;
+                            if (cur == kEmpty) {
+                                uint32_t prev = atomicCAS(ks + s, kEmpty, c);
+                                if (prev == kEmpty || prev == c) break;
+                            }
+                            s = (s + 1) & (S - 1);
+                        }
+                        atomicAdd(vs + s, ww[b]);
+                    }
+                } else if (jj[b] != i) {
+                    e_part += ww[b];
+                } else {
+                    s_part += ww[b];
+                }
+            }
+        }
+        e_part = warp_sum(e_part);
+        s_part = warp_sum(s_part);
+        if ((threadIdx.x & 31) == 0) {
+            if (e_part != 0) atomicAdd(rank_ptr<CS>(&acc_e[par], 0), e_part);
+            if (s_part != 0) atomicAdd(rank_ptr<CS>(&acc_s[par], 0), s_part);
+        }
+        cluster_barrier<CS>();  // all inserts and partial sums are in
+        const double e_src = *rank_ptr<CS>(&acc_e[par], 0);
+        G best = G(0);
+        uint32_t dst = src;
+        for (int s0 = threadIdx.x; s0 < S; s0 += kClusterThreads * EB) {
+            uint32_t kk[EB];
+            double kv[EB], sc[EB];
+#pragma unroll
+            for (int b = 0; b < EB; b++) {
+                const int s = s0 + b * kClusterThreads;
+                kk[b] = kEmpty;
+                if (s < S) {
+                    if constexpr (kIntg<WK>) {
+                        uint64_t v = packed[s];
+                        kk[b] = (uint32_t)(v >> 32);
+                        kv[b] = u2d((uint32_t)v);
+                        if (kk[b] != kEmpty) packed[s] = kEmpty64;
+                    } else {
+                        kk[b] = keys[s];
+                        if (kk[b] != kEmpty) {
+                            kv[b] = vals[s];
+                            keys[s] = kEmpty;
+                            vals[s] = 0.0;
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < EB; b++)
+                if (kk[b] != kEmpty) sc[b] = A.sigma[kk[b]];
+#pragma unroll
+            for (int b = 0; b < EB; b++) {
+                if (kk[b] != kEmpty) {
+                    G gn = Prec<PREC>::gain(kv[b], e_src, ki, a, sc[b], A);
+                    if (better(gn, kk[b], best, dst, A.up)) {
+                        best = gn;
+                        dst = kk[b];
+                    }
+                    dcnt++;
+                }
+            }
+        }
+        group_argmax<kClusterThreads, G>(best, dst, A.up, red_g, red_c);
+        if (threadIdx.x == 0) {
+            rank_ptr<CS>(&best_g[par][0], 0)[rank] = best;
+            rank_ptr<CS>(&best_c[par][0], 0)[rank] = dst;
+        }
+        cluster_barrier<CS>();  // winners of every CTA are with rank 0
+        if (rank == 0 && threadIdx.x == 0) {
+            G bg = G(0);
+            uint32_t bc = src;
+            for (int r = 0; r < CS; r++)
+                if (better(best_g[par][r], best_c[par][r], bg, bc, A.up)) {
+                    bg = best_g[par][r];
+                    bc = best_c[par][r];
+                }
+            A.N[i] = final_choice<VER>(bc, src, A.up);
+            sin += e_src + acc_s[par];
+            acc_e[par] = 0;
+            acc_s[par] = 0;
+        }
+    }
+    cluster_barrier<CS>();  // no CTA leaves while others may still touch its memory
+    flush_acc(A.acc, A.integral, sin, dcnt);
+}
+
+// ============================================================================
+// bin 9, last tier (giants): global tables, many CTAs per vertex
 // ============================================================================
 constexpr int kHeavyThreads = 256;
 constexpr uint32_t kHeavyChunkE = 4096;  // edges per insert item
@@ -460,6 +675,11 @@ __device__ __forceinline__ uint32_t find_item(const uint32_t *item_off, uint32_t
         else hi = mid;
     }
     return lo;
+}
+
+__global__ void heavy_degree_kernel(const uint32_t *off, const uint32_t *hv, uint32_t H, uint32_t *deg) {
+    uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h < H) deg[h] = off[hv[h] + 1] - off[hv[h]];
 }
 
 __global__ void heavy_layout_kernel(const uint32_t *off, const uint32_t *hv, uint32_t H, uint32_t *tsize,
@@ -501,7 +721,7 @@ __global__ void __launch_bounds__(kHeavyThreads) heavy_insert_kernel(LMArgs A, c
 #pragma unroll
         for (int b = 0; b < BATCH; b++) {
             uint32_t e = base + b * kHeavyThreads;
-            jj[b] = e < hi ? __ldg(A.col + e) : kEmpty;
+            jj[b] = e < hi ? __ldcs(A.col + e) : kEmpty;
             ww[b] = e < hi ? wload<WK>(A.w, e) : 0.0;
         }
 #pragma unroll
@@ -703,6 +923,67 @@ __global__ void level_init_kernel(const uint32_t *off, const void *w, uint32_t n
     }
 }
 
+template <int CS, int WK, int PREC, int VER>
+size_t cluster_smem() {
+    return (size_t)kClusterSlots * (kIntg<WK> ? sizeof(uint64_t) : sizeof(uint32_t) + sizeof(double));
+}
+
+template <int CS, int WK, int PREC, int VER>
+cudaLaunchConfig_t cluster_config(size_t smem, unsigned grid, cudaStream_t s, cudaLaunchAttribute *attr) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid, 1, 1);
+    cfg.blockDim = dim3(kClusterThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CS;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+// Maximum co-resident clusters of a cluster kernel (0 when the shape cannot run).
+template <int CS, int WK, int PREC, int VER>
+int cluster_capacity() {
+    static int cap = -1;
+    if (cap >= 0) return cap;
+    auto kern = lm_cluster_kernel<CS, WK, PREC, VER>;
+    const size_t smem = cluster_smem<CS, WK, PREC, VER>();
+    MG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (CS > 8) MG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = cluster_config<CS, WK, PREC, VER>(smem, CS * 148, nullptr, attr);
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, (void *)kern, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    cap = n;
+    return cap;
+}
+
+template <int CS, int WK, int PREC, int VER>
+void launch_cluster(const LMArgs &A, const uint32_t *verts, uint32_t count, cudaStream_t s) {
+    auto kern = lm_cluster_kernel<CS, WK, PREC, VER>;
+    const size_t smem = cluster_smem<CS, WK, PREC, VER>();
+    int cap = cluster_capacity<CS, WK, PREC, VER>();
+    MG_CHECK(cap > 0, MG_ERR_UNSUPPORTED, "cluster shape cannot be scheduled on this device");
+    unsigned clusters = (unsigned)std::min<uint64_t>(count, (uint64_t)cap);
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = cluster_config<CS, WK, PREC, VER>(smem, clusters * CS, s, attr);
+    MG_CUDA(cudaLaunchKernelEx(&cfg, kern, A, verts, count));
+    MG_LAUNCH_CHECK();
+}
+
+// Largest cluster size (8 or 16) the device schedules for the heavy tiers.
+int probe_max_cluster() {
+    return cluster_capacity<16, WK_F64, MG_PREC_FP64, 2>() > 0 && cluster_capacity<16, WK_UNIT, MG_PREC_FP64, 2>() > 0
+               ? 16
+               : 8;
+}
+
 template <int WK, int PREC, int VER>
 void launch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, const LMArgs &A, cudaStream_t s) {
     const Bins &B = lvl.bins;
@@ -710,9 +991,20 @@ void launch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, c
     MG_CUDA(cudaEventRecord(ws.ev_fork, s));
     for (int q = 0; q < 3; q++) MG_CUDA(cudaStreamWaitEvent(ws.streams[q], ws.ev_fork, 0));
     cudaStream_t sh = ws.streams[0], sm = ws.streams[1], st = ws.streams[2];
-    if (lvl.heavy > 0) {
-        const uint32_t H = lvl.heavy;
-        const uint32_t *hv = ws.perm.get() + B.offset[9];
+    // heavy tiers, largest clusters first
+    if (lvl.tier_off[5] > lvl.tier_off[4])
+        launch_cluster<16, WK, PREC, VER>(A, ws.h_tier.get() + lvl.tier_off[4], lvl.tier_off[5] - lvl.tier_off[4], sh);
+    if (lvl.tier_off[4] > lvl.tier_off[3])
+        launch_cluster<8, WK, PREC, VER>(A, ws.h_tier.get() + lvl.tier_off[3], lvl.tier_off[4] - lvl.tier_off[3], sh);
+    if (lvl.tier_off[3] > lvl.tier_off[2])
+        launch_cluster<4, WK, PREC, VER>(A, ws.h_tier.get() + lvl.tier_off[2], lvl.tier_off[3] - lvl.tier_off[2], sh);
+    if (lvl.tier_off[2] > lvl.tier_off[1])
+        launch_cluster<2, WK, PREC, VER>(A, ws.h_tier.get() + lvl.tier_off[1], lvl.tier_off[2] - lvl.tier_off[1], sh);
+    if (lvl.tier_off[1] > lvl.tier_off[0])
+        launch_cluster<1, WK, PREC, VER>(A, ws.h_tier.get() + lvl.tier_off[0], lvl.tier_off[1] - lvl.tier_off[0], sm);
+    if (lvl.giants > 0) {
+        const uint32_t H = lvl.giants;
+        const uint32_t *hv = ws.h_tier.get() + lvl.tier_off[kTiers - 1];
         heavy_insert_kernel<WK, VER><<<lvl.ins_items, kHeavyThreads, 0, sh>>>(
             A, hv, H, ws.h_ins.get(), ws.h_toff.get(), ws.h_tsize.get(), ws.h_keys.get(), ws.h_vals.get(),
             ws.h_acc.get());
@@ -781,9 +1073,47 @@ void move_prepare_level(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, c
     lvl.heavy = lvl.bins.size[9];
     lvl.ins_items = lvl.eval_items = 0;
     lvl.table_slots = 0;
+    lvl.giants = 0;
+    for (int t = 0; t <= kTiers; t++) lvl.tier_off[t] = 0;
     if (lvl.heavy == 0) return;
-    const uint32_t H = lvl.heavy;
-    const uint32_t *hv = perm + lvl.bins.offset[9];
+    if (ws.max_cluster == 0) ws.max_cluster = probe_max_cluster();
+    // tiers by degree: tier t (cluster of 2^t CTAs) takes deg <= 2^t * S / 2
+    {
+        const uint32_t Hall = lvl.heavy;
+        const uint32_t *hall = perm + lvl.bins.offset[9];
+        uint32_t *deg = ws.h_deg.ensure(Hall + 1);
+        heavy_degree_kernel<<<(unsigned)ceil_div(Hall, 256), 256, 0, s>>>(g.off, hall, Hall, deg);
+        MG_LAUNCH_CHECK();
+        std::vector<uint32_t> hv_h(Hall), dg_h(Hall);
+        MG_CUDA(cudaMemcpyAsync(hv_h.data(), hall, sizeof(uint32_t) * Hall, cudaMemcpyDeviceToHost, s));
+        MG_CUDA(cudaMemcpyAsync(dg_h.data(), deg, sizeof(uint32_t) * Hall, cudaMemcpyDeviceToHost, s));
+        MG_CUDA(cudaStreamSynchronize(s));
+        std::vector<uint32_t> lists[kTiers];
+        const int top = ws.max_cluster >= 16 ? 4 : 3;
+        for (uint32_t h = 0; h < Hall; h++) {
+            int t = kTiers - 1;
+            for (int c = 0; c <= top; c++)
+                if ((uint64_t)dg_h[h] <= (uint64_t)(kClusterSlots / 2) << c) {
+                    t = c;
+                    break;
+                }
+            lists[t].push_back(hv_h[h]);
+        }
+        std::vector<uint32_t> tiered;
+        tiered.reserve(Hall);
+        for (int t = 0; t < kTiers; t++) {
+            lvl.tier_off[t] = (uint32_t)tiered.size();
+            tiered.insert(tiered.end(), lists[t].begin(), lists[t].end());
+        }
+        lvl.tier_off[kTiers] = (uint32_t)tiered.size();
+        MG_CUDA(cudaMemcpyAsync(ws.h_tier.ensure(Hall + 1), tiered.data(), sizeof(uint32_t) * Hall,
+                                cudaMemcpyHostToDevice, s));
+        lvl.giants = lvl.tier_off[kTiers] - lvl.tier_off[kTiers - 1];
+        MG_CUDA(cudaStreamSynchronize(s));
+    }
+    if (lvl.giants == 0) return;
+    const uint32_t H = lvl.giants;
+    const uint32_t *hv = ws.h_tier.get() + lvl.tier_off[kTiers - 1];
     uint32_t *tsize = ws.h_tsize.ensure(H + 1);
     uint32_t *ins = ws.h_ins.ensure(H + 1);
     uint32_t *ev = ws.h_eval.ensure(H + 1);
@@ -828,7 +1158,13 @@ void move_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, con
     A.sigma = sigma;
     A.perm = ws.perm.get();
     A.m = p.mass / 2.0;
+    A.two_m = 2.0 * A.m;
+    A.r_m = 1.0 / A.m;
+    A.r_two_m = 1.0 / A.two_m;
     A.m_f = (float)(p.mass / 2.0);
+    A.two_m_f = 2.0f * A.m_f;
+    A.r_m_f = 1.0f / A.m_f;
+    A.r_two_m_f = 1.0f / A.two_m_f;
     A.mass_i = (long long)p.mass;
     A.up = p.up;
     A.integral = p.integral;
@@ -837,19 +1173,25 @@ void move_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, con
     if (p.precision == MG_PREC_INT64)
         MG_CHECK(p.integral && p.mass < 2147483648.0, MG_ERR_UNSUPPORTED,
                  "int64 precision needs integral weights with total below 2^31");
+    // integral graphs accumulate in integer table slots
+    const int wk = p.integral ? (g.wk == WK_F32 ? (int)WK_F32I : g.wk == WK_F64 ? (int)WK_F64I : g.wk) : g.wk;
 #define MG_SWEEP_CASE(WKV, PRECV)                                                                  \
-    if (g.wk == WKV && p.precision == PRECV) {                                                     \
+    if (wk == WKV && p.precision == PRECV) {                                                       \
         if (p.version == 1) launch_sweep<WKV, PRECV, 1>(g, lvl, ws, A, s);                         \
         else launch_sweep<WKV, PRECV, 2>(g, lvl, ws, A, s);                                        \
         return;                                                                                    \
     }
     MG_SWEEP_CASE(WK_UNIT, MG_PREC_FP64)
+    MG_SWEEP_CASE(WK_F32I, MG_PREC_FP64)
+    MG_SWEEP_CASE(WK_F64I, MG_PREC_FP64)
     MG_SWEEP_CASE(WK_F32, MG_PREC_FP64)
     MG_SWEEP_CASE(WK_F64, MG_PREC_FP64)
     MG_SWEEP_CASE(WK_UNIT, MG_PREC_INT64)
-    MG_SWEEP_CASE(WK_F32, MG_PREC_INT64)
-    MG_SWEEP_CASE(WK_F64, MG_PREC_INT64)
+    MG_SWEEP_CASE(WK_F32I, MG_PREC_INT64)
+    MG_SWEEP_CASE(WK_F64I, MG_PREC_INT64)
     MG_SWEEP_CASE(WK_UNIT, MG_PREC_FP32)
+    MG_SWEEP_CASE(WK_F32I, MG_PREC_FP32)
+    MG_SWEEP_CASE(WK_F64I, MG_PREC_FP32)
     MG_SWEEP_CASE(WK_F32, MG_PREC_FP32)
     MG_SWEEP_CASE(WK_F64, MG_PREC_FP32)
 #undef MG_SWEEP_CASE

@@ -121,7 +121,7 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
         double lm = tp.stop_sync();
         phase_lm += lm;
         account_sweep(ctx, cur, hacc, S);
-        S.iterations++;
+        S.sweeps++;
         S.edges_swept += cur.nnz;
         S.distinct_pairs += hacc.distinct;
         if (phase == 0) {
@@ -145,7 +145,7 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
             double dt = ti.stop_sync();
             phase_lm += dt;
             account_sweep(ctx, cur, hacc, S);
-            S.iterations++;
+            S.sweeps++;
             S.edges_swept += cur.nnz;
             S.distinct_pairs += hacc.distinct;
             if (phase == 0) S.phase0_edges_swept += cur.nnz;
@@ -164,6 +164,7 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
                 break;
             }
         }
+        S.iterations += loop;  // the reference's loop count (moves evaluated)
         S.seconds_local_move += phase_lm;
         if (phase == 0) S.phase0_seconds = phase_lm;
         if (verbose) {

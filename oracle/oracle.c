@@ -892,3 +892,29 @@ double or_time_phase0(const or_graph *g, int version, int iters, uint64_t *edges
     if (edges_done) *edges_done = (uint64_t)iters * g->nnz;
     return t1 - t0;
 }
+
+/* ======================================================================== */
+/* Check of the engine's division by a run constant: for divisor d with      */
+/* r = RN(1/d), q0 = RN(x*r), rem = fma(-q0, d, x), q = fma(rem, r, q0)      */
+/* equals RN(x/d) (Markstein's theorem).  Counts mismatches over n inputs   */
+/* x drawn from the gain's value range for each divisor.                    */
+/* ======================================================================== */
+uint64_t or_check_const_division(uint64_t n, uint64_t seed, const double *divisors, int nd) {
+    uint64_t bad = 0;
+#pragma omp parallel for schedule(static) reduction(+ : bad)
+    for (uint64_t i = 0; i < n; i++) {
+        uint64_t h = or_mix64(seed + i);
+        double d = divisors[i % (uint64_t)nd];
+        double r = 1.0 / d;
+        /* x: random mantissa, exponent spread over +-2^60 around d, both signs */
+        int ex = (int)((h >> 52) % 121) - 60;
+        double m = 1.0 + (double)(h & 0xFFFFFFFFFFFFFull) / 4503599627370496.0;
+        double x = ldexp(m, ex) * d * ((h >> 63) ? -1.0 : 1.0);
+        if (i % 7 == 0) x = (double)(int64_t)(h % 4000000000ull) - 2000000000.0; /* integers */
+        double q0 = x * r;
+        double rem = fma(-q0, d, x);
+        double q = fma(rem, r, q0);
+        if (q != x / d) bad++;
+    }
+    return bad;
+}

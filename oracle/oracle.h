@@ -110,6 +110,9 @@ int or_louvain(const or_graph *g, int version, double threshold, int max_phases,
  * phase 0 and return seconds spent (for the CPU baseline). */
 double or_time_phase0(const or_graph *g, int version, int iters, uint64_t *edges_done);
 
+/* mismatches of the reciprocal-plus-fma division against x/d (test helper) */
+uint64_t or_check_const_division(uint64_t n, uint64_t seed, const double *divisors, int nd);
+
 #ifdef __cplusplus
 }
 #endif

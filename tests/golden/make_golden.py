@@ -42,7 +42,7 @@ def write_mtx(path, g, weighted):
             f.write("%%MatrixMarket matrix coordinate real general\n")
             f.write(f"{g.n} {g.n} {int(m.sum())}\n")
             for r, c, w in zip(row[m], g.cols[m], g.weights[m]):
-                f.write(f"{r + 1} {c + 1} {w!r}\n")
+                f.write(f"{r + 1} {c + 1} {float(w)!r}\n")
         else:
             f.write("%%MatrixMarket matrix coordinate pattern symmetric\n")
             f.write(f"{g.n} {g.n} {int(m.sum())}\n")

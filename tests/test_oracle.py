@@ -185,3 +185,16 @@ def test_loader_rules(O, tmp_path):
     bad.write_text("%%MatrixMarket matrix coordinate pattern symmetric\n3 3 2\n2 1\n")
     with pytest.raises(ValueError):
         O.load_mtx(str(bad))
+
+
+def test_constant_division_identity(O):
+    """The engine divides by m and 2m with a precomputed reciprocal and one fma
+    correction; this checks the identity against IEEE division on the CPU."""
+    import ctypes as ct
+    L = O.lib()
+    L.or_check_const_division.restype = ct.c_uint64
+    L.or_check_const_division.argtypes = [ct.c_uint64, ct.c_uint64, ct.c_void_p, ct.c_int]
+    rng = np.random.default_rng(3)
+    d = np.ascontiguousarray(np.concatenate([[1.0, 2.0, 3.0, 520770236.0, 260385118.0, 521211.0],
+                                             rng.uniform(1, 4e9, 64), rng.integers(1, 2**32, 64).astype(float)]))
+    assert L.or_check_const_division(4_000_000, 11, d.ctypes.data, len(d)) == 0
