@@ -122,6 +122,29 @@ mg_status mg_bins_offsets(mg_ctx *ctx, int scheme, uint32_t n, const uint64_t *o
 mg_status mg_local_move(mg_graph *g, int version, int up, int precision, const uint32_t *C,
                         const double *sigma, const double *k, uint32_t *C_new, uint64_t *distinct);
 
+/* One local-move sweep that allocates nothing.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc, such as a
+ * serving process that has handed its whole HBM budget to its own pool, or
+ * code that must not enter the CUDA allocator.  Everything is in device
+ * memory owned by the caller: the CSR (d_offsets[n+1] as uint32, d_cols,
+ * d_weights or NULL for unit weights), the assignment d_C, sigma d_sigma, vertex
+ * weights d_k (n each) and the output d_C_new (n).  mass = sum of all
+ * weights.  Results equal mg_local_move (FP64 gains) for integral weights.
+ * Work is queued on `stream` (a cudaStream_t, NULL = default stream); the call
+ * waits for the stream once, to read the graph's maximum degree.
+ * Scratch: the per-block hash tables live in one static 16 MiB device array
+ * that every GPU loading the library holds until exit.  A graph whose
+ * maximum degree needs a table beyond it (a degree above 524,287) is rejected
+ * with MG_ERR_UNSUPPORTED.  The first call on a device looks up
+ * that array's device address (a one-time set-up per device); make that first
+ * call before any stream capture.  All calls share the array and clear it on
+ * entry, so calls that overlap on the GPU race with each other.  Errors are
+ * reported by mg_last_error(NULL). */
+mg_status mg_local_move_noalloc(uint32_t n, const uint32_t *d_offsets, const uint32_t *d_cols,
+                                const double *d_weights, double mass, const uint32_t *d_C,
+                                const double *d_sigma, const double *d_k, uint32_t *d_C_new,
+                                int version, int up, void *stream);
+
 /* Modularity of an assignment (src/louvain/louvain.cu:105-238), sigma_tot
  * computed from C. */
 mg_status mg_modularity(mg_graph *g, const uint32_t *C, double *q);

@@ -59,6 +59,9 @@ mg_ctx::~mg_ctx() {
 namespace mg {
 thread_local unsigned long long g_kernel_launches = 0;
 
+// error text for entry points that run without a context (mg_last_error(NULL))
+void set_orphan_error(const std::string &msg) { g_orphan_error = msg; }
+
 void ctx_prepare(mg_ctx *ctx) {
     if (ctx->stream) return;
     MG_CUDA(cudaSetDevice(ctx->device));
