@@ -335,6 +335,7 @@ mg_status mg_local_move(mg_graph *g, int version, int up, int precision, const u
         MG_CUDA(cudaMemcpyAsync(C_new, dN, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
         MG_CUDA(cudaMemcpyAsync(ctx->h_acc, ctx->mws.acc.get(), sizeof(SweepAcc), cudaMemcpyDeviceToHost, s));
         MG_CUDA(cudaStreamSynchronize(s));
+        MG_CHECK(ctx->h_acc->overflow == 0, MG_ERR_UNSUPPORTED, "local move: a cluster hash segment overflowed");
         if (distinct) *distinct = ctx->h_acc->distinct;
     });
 }

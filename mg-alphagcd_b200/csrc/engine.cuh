@@ -43,7 +43,8 @@ struct SweepAcc {
     unsigned long long moved;     // vertices whose community changed
     double sin_f;                 // same sums for real weights
     double s2_f;
-    double pad[2];
+    unsigned long long overflow;  // inserts that found no free slot (must stay 0)
+    double pad;
 };
 
 // Heavy vertices (last bin) are split into tiers by degree: tier t < 5 is

@@ -264,6 +264,31 @@ __device__ __forceinline__ void group_sync() {
     else __syncthreads();
 }
 
+// Two sums over a group of GT threads with one pair of barriers; results
+// valid in every thread.  red: 2 * 32 doubles.
+template <int GT>
+__device__ __forceinline__ void group_sum2(double &a, double &b, double *red) {
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if constexpr (GT > 32) {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (lane == 0) {
+            red[warp] = a;
+            red[32 + warp] = b;
+        }
+        __syncthreads();
+        double ta = 0, tb = 0;
+#pragma unroll
+        for (int w2 = 0; w2 < GT / 32; w2++) {
+            ta += red[w2];
+            tb += red[32 + w2];
+        }
+        __syncthreads();
+        a = ta;
+        b = tb;
+    }
+}
+
 // Sum over a group of GT threads; result valid in every thread.
 template <int GT>
 __device__ __forceinline__ double group_sum(double v, double *red) {
@@ -344,24 +369,54 @@ __device__ __forceinline__ int table_bits(uint32_t d) {
     return want < Log2<SLOTS>::value ? want : Log2<SLOTS>::value;
 }
 
+// weight of edge e as the table's value type: exact 32-bit integer for
+// integral graphs (no float->int conversion instruction: the f64 value plus
+// 2^52 carries the integer in its low mantissa word), double otherwise
+template <int WK>
+__device__ __forceinline__ typename ValT<WK>::type wget(const void *w, uint32_t e) {
+    if constexpr (WK == WK_UNIT) return 1u;
+    else if constexpr (WK == WK_F64I)
+        return (uint32_t)__double2loint(__dadd_rn(__ldcs((const double *)w + e), 4503599627370496.0));
+    else if constexpr (WK == WK_F32I) return __float2uint_rn(__ldcs((const float *)w + e));
+    else return wload<WK>(w, e);
+}
+
+template <class V>
+__device__ __forceinline__ double v2d(V v) {
+    if constexpr (std::is_same<V, uint32_t>::value) return u2d(v);
+    else return v;
+}
+
+// Shared-memory hash table per group of GT threads.  Newly inserted slots are
+// appended to a per-table list, so the evaluation runs densely over the
+// distinct candidates only (and resets exactly those slots).
 template <int GT, int SLOTS, int WK, int PREC, int VER, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) lm_hash_kernel(LMArgs A, uint32_t bin_off, uint32_t bin_size) {
     using G = typename Prec<PREC>::G;
     using V = typename ValT<WK>::type;
     constexpr int GPB = BLOCK / GT;
     constexpr int BATCH = 4;
+    constexpr int EB = 4;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t *keys_all = (uint32_t *)smem_raw;
     V *vals_all = (V *)(smem_raw + sizeof(uint32_t) * SLOTS * GPB);
-    __shared__ double red_d[32];
+    uint16_t *used_all = (uint16_t *)(smem_raw + (sizeof(uint32_t) + sizeof(V)) * SLOTS * GPB);
+    __shared__ V acc_e[GPB], acc_s[GPB];
+    __shared__ uint32_t cnt[GPB];
     __shared__ G red_g[32];
     __shared__ uint32_t red_c[32];
     const int g = threadIdx.x / GT, t = threadIdx.x % GT;
     uint32_t *keys = keys_all + g * SLOTS;
     V *vals = vals_all + g * SLOTS;
+    uint16_t *used = used_all + g * (SLOTS / 2);
     for (int s2 = threadIdx.x; s2 < SLOTS * GPB; s2 += BLOCK) {
         keys_all[s2] = kEmpty;
         vals_all[s2] = V(0);
+    }
+    if (threadIdx.x < GPB) {
+        acc_e[threadIdx.x] = V(0);
+        acc_s[threadIdx.x] = V(0);
+        cnt[threadIdx.x] = 0;
     }
     __syncthreads();
     double sin = 0;
@@ -380,16 +435,15 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) lm_hash_kernel(LMArgs A, 
             a = A.sigma[src] - ki;  // issued early, consumed after the edge pass
         }
         const int tb = table_bits<SLOTS>(hi - lo);
-        const int tsz = 1 << tb;
-        double e_part = 0, s_part = 0;
+        V e_part = V(0), s_part = V(0);
         for (uint32_t base = lo + t; base < hi; base += GT * BATCH) {
             uint32_t jj[BATCH], cc[BATCH];
-            double ww[BATCH];
+            V ww[BATCH];
 #pragma unroll
             for (int b = 0; b < BATCH; b++) {
                 uint32_t e = base + b * GT;
                 jj[b] = e < hi ? __ldcs(A.col + e) : kEmpty;
-                ww[b] = e < hi ? wload<WK>(A.w, e) : 0.0;
+                ww[b] = e < hi ? wget<WK>(A.w, e) : V(0);
             }
 #pragma unroll
             for (int b = 0; b < BATCH; b++) cc[b] = jj[b] != kEmpty ? A.P[jj[b]] : kEmpty;
@@ -399,9 +453,22 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) lm_hash_kernel(LMArgs A, 
                 const uint32_t c = cc[b];
                 if (c != src) {
                     if (is_candidate<VER>(c, src, A.up)) {
-                        uint32_t h = table_find_or_insert<SLOTS>(keys, c, tb);
-                        if constexpr (kIntg<WK>) atomicAdd(vals + h, (uint32_t)ww[b]);
-                        else atomicAdd(vals + h, ww[b]);
+                        const uint32_t mask = (1u << tb) - 1u;
+                        uint32_t h = hash_slot(c, tb);
+                        for (int p = 0; p < SLOTS; p++) {
+                            uint32_t cur = ((volatile uint32_t *)keys)[h];
+                            if (cur == c) break;
+                            if (cur == kEmpty) {
+                                uint32_t prev = atomicCAS(keys + h, kEmpty, c);
+                                if (prev == kEmpty) {
+                                    used[atomicAdd(cnt + g, 1u)] = (uint16_t)h;
+                                    break;
+                                }
+                                if (prev == c) break;
+                            }
+                            h = (h + 1) & mask;
+                        }
+                        atomicAdd(vals + h, ww[b]);
                     }
                 } else if (jj[b] != i) {
                     e_part += ww[b];
@@ -410,32 +477,37 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) lm_hash_kernel(LMArgs A, 
                 }
             }
         }
+        // group totals of e and self weight, folded into the barrier that
+        // publishes the table
+        e_part = warp_sum(e_part);
+        s_part = warp_sum(s_part);
+        if ((threadIdx.x & 31) == 0) {
+            if (e_part != V(0)) atomicAdd(acc_e + g, e_part);
+            if (s_part != V(0)) atomicAdd(acc_s + g, s_part);
+        }
         group_sync<GT>();
-        const double e_src = group_sum<GT>(e_part, red_d);
-        const double selfw = group_sum<GT>(s_part, red_d);
+        const double e_src = v2d(acc_e[g]), selfw = v2d(acc_s[g]);
+        const uint32_t nd = cnt[g];
         G best = G(0);
         uint32_t dst = src;
-        // every slot of this thread in one batch, so the sigma gathers overlap
-        constexpr int EB = SLOTS / GT < 8 ? SLOTS / GT : 8;
-        for (int s0 = t; s0 < tsz; s0 += GT * EB) {
+        for (uint32_t u0 = t; u0 < nd; u0 += GT * EB) {
             uint32_t kk[EB];
             double sc[EB], kv[EB];
 #pragma unroll
             for (int b = 0; b < EB; b++) {
-                int s2 = s0 + b * GT;
-                kk[b] = s2 < tsz ? keys[s2] : kEmpty;
-            }
-#pragma unroll
-            for (int b = 0; b < EB; b++) {
-                int s2 = s0 + b * GT;
-                if (kk[b] != kEmpty) {
-                    sc[b] = A.sigma[kk[b]];
-                    if constexpr (kIntg<WK>) kv[b] = u2d(vals[s2]);
-                    else kv[b] = (double)vals[s2];
-                    keys[s2] = kEmpty;
-                    vals[s2] = V(0);
+                const uint32_t u = u0 + b * GT;
+                kk[b] = kEmpty;
+                if (u < nd) {
+                    const uint32_t h = used[u];
+                    kk[b] = keys[h];
+                    kv[b] = v2d(vals[h]);
+                    keys[h] = kEmpty;
+                    vals[h] = V(0);
                 }
             }
+#pragma unroll
+            for (int b = 0; b < EB; b++)
+                if (kk[b] != kEmpty) sc[b] = A.sigma[kk[b]];
 #pragma unroll
             for (int b = 0; b < EB; b++) {
                 if (kk[b] != kEmpty) {
@@ -444,14 +516,19 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) lm_hash_kernel(LMArgs A, 
                         best = gn;
                         dst = kk[b];
                     }
-                    dcnt++;
                 }
             }
         }
         group_argmax<GT, G>(best, dst, A.up, red_g, red_c);
-        if (active && t == 0) {
-            A.N[i] = final_choice<VER>(dst, src, A.up);
-            sin += e_src + selfw;
+        if (t == 0) {
+            if (active) {
+                A.N[i] = final_choice<VER>(dst, src, A.up);
+                sin += e_src + selfw;
+                dcnt += nd;
+            }
+            cnt[g] = 0;
+            acc_e[g] = V(0);
+            acc_s[g] = V(0);
         }
         group_sync<GT>();
     }
@@ -468,7 +545,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) lm_hash_kernel(LMArgs A, 
 // Unit weights use packed 64-bit slots {key:32 | count:32}.
 // ============================================================================
 namespace cg = cooperative_groups;
-constexpr int kClusterThreads = 1024;
+constexpr int kClusterThreads = 1024;  // one CTA per SM with a 16K-slot segment
 constexpr uint64_t kEmpty64 = 0xFFFFFFFF00000000ull;
 
 template <int CS>
@@ -494,6 +571,9 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
     uint64_t *packed = (uint64_t *)smem_raw;                 // integral weights
     uint32_t *keys = (uint32_t *)smem_raw;                   // real weights
     double *vals = (double *)(smem_raw + sizeof(uint32_t) * S);
+    // slots of this CTA's segment that received a new key, in insertion order
+    uint16_t *used = (uint16_t *)(smem_raw + (kIntg<WK> ? sizeof(uint64_t) : sizeof(uint32_t) + sizeof(double)) * S);
+    __shared__ uint32_t ucnt;
     __shared__ double acc_e[2], acc_s[2];
     __shared__ G best_g[2][CS];
     __shared__ uint32_t best_c[2][CS];
@@ -512,6 +592,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
         acc_e[threadIdx.x] = 0;
         acc_s[threadIdx.x] = 0;
     }
+    if (threadIdx.x == 0) ucnt = 0;
     cluster_barrier<CS>();
     const uint32_t cluster_id = blockIdx.x / CS, nclusters = gridDim.x / CS;
     const uint32_t tc = rank * kClusterThreads + threadIdx.x;
@@ -548,37 +629,60 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
                     if constexpr (kIntg<WK>) {
                         const unsigned long long wi = (uint32_t)ww[b];
                         uint64_t *seg = rank_ptr<CS>(packed, owner);
+                        bool placed = false;
                         for (int p = 0; p < S; p++) {
                             uint64_t cur = ((volatile uint64_t *)seg)[s];
                             uint32_t k = (uint32_t)(cur >> 32);
                             if (k == c) {
                                 atomicAdd((unsigned long long *)(seg + s), wi);
+                                placed = true;
                                 break;
                             }
                             if (k == kEmpty) {
                                 uint64_t prev = atomicCAS((unsigned long long *)(seg + s), kEmpty64,
                                                           ((uint64_t)c << 32) | wi);
-                                if (prev == kEmpty64) break;
+                                if (prev == kEmpty64) {
+                                    rank_ptr<CS>(used, owner)[atomicAdd(rank_ptr<CS>(&ucnt, owner), 1u)] =
+                                        (uint16_t)s;
+                                    placed = true;
+                                    break;
+                                }
                                 if ((uint32_t)(prev >> 32) == c) {
                                     atomicAdd((unsigned long long *)(seg + s), wi);
+                                    placed = true;
                                     break;
                                 }
                             }
                             s = (s + 1) & (S - 1);
                         }
+                        if (!placed) atomicAdd(&A.acc->overflow, 1ull);
                     } else {
                         uint32_t *ks = rank_ptr<CS>(keys, owner);
                         double *vs = rank_ptr<CS>(vals, owner);
+                        bool placed = false;
                         for (int p = 0; p < S; p++) {
                             uint32_t cur = ((volatile uint32_t *)ks)[s];
-                            if (cur == c) break;
+                            if (cur == c) {
+                                placed = true;
+                                break;
+                            }
                             if (cur == kEmpty) {
                                 uint32_t prev = atomicCAS(ks + s, kEmpty, c);
-                                if (prev == kEmpty || prev == c) break;
+                                if (prev == kEmpty) {
+                                    rank_ptr<CS>(used, owner)[atomicAdd(rank_ptr<CS>(&ucnt, owner), 1u)] =
+                                        (uint16_t)s;
+                                    placed = true;
+                                    break;
+                                }
+                                if (prev == c) {
+                                    placed = true;
+                                    break;
+                                }
                             }
                             s = (s + 1) & (S - 1);
                         }
-                        atomicAdd(vs + s, ww[b]);
+                        if (placed) atomicAdd(vs + s, ww[b]);
+                        else atomicAdd(&A.acc->overflow, 1ull);
                     }
                 } else if (jj[b] != i) {
                     e_part += ww[b];
@@ -597,26 +701,26 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
         const double e_src = *rank_ptr<CS>(&acc_e[par], 0);
         G best = G(0);
         uint32_t dst = src;
-        for (int s0 = threadIdx.x; s0 < S; s0 += kClusterThreads * EB) {
+        const uint32_t nd = ucnt;
+        for (uint32_t u0 = threadIdx.x; u0 < nd; u0 += kClusterThreads * EB) {
             uint32_t kk[EB];
             double kv[EB], sc[EB];
 #pragma unroll
             for (int b = 0; b < EB; b++) {
-                const int s = s0 + b * kClusterThreads;
+                const uint32_t u = u0 + b * kClusterThreads;
                 kk[b] = kEmpty;
-                if (s < S) {
+                if (u < nd) {
+                    const uint32_t s = used[u];
                     if constexpr (kIntg<WK>) {
                         uint64_t v = packed[s];
                         kk[b] = (uint32_t)(v >> 32);
                         kv[b] = u2d((uint32_t)v);
-                        if (kk[b] != kEmpty) packed[s] = kEmpty64;
+                        packed[s] = kEmpty64;
                     } else {
                         kk[b] = keys[s];
-                        if (kk[b] != kEmpty) {
-                            kv[b] = vals[s];
-                            keys[s] = kEmpty;
-                            vals[s] = 0.0;
-                        }
+                        kv[b] = vals[s];
+                        keys[s] = kEmpty;
+                        vals[s] = 0.0;
                     }
                 }
             }
@@ -631,12 +735,13 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
                         best = gn;
                         dst = kk[b];
                     }
-                    dcnt++;
                 }
             }
         }
         group_argmax<kClusterThreads, G>(best, dst, A.up, red_g, red_c);
         if (threadIdx.x == 0) {
+            dcnt += nd;
+            ucnt = 0;  // every thread of this CTA has read it (barriers in group_argmax)
             rank_ptr<CS>(&best_g[par][0], 0)[rank] = best;
             rank_ptr<CS>(&best_c[par][0], 0)[rank] = dst;
         }
@@ -925,7 +1030,7 @@ __global__ void level_init_kernel(const uint32_t *off, const void *w, uint32_t n
 
 template <int CS, int WK, int PREC, int VER>
 size_t cluster_smem() {
-    return (size_t)kClusterSlots * (kIntg<WK> ? sizeof(uint64_t) : sizeof(uint32_t) + sizeof(double));
+    return (size_t)kClusterSlots * ((kIntg<WK> ? sizeof(uint64_t) : sizeof(uint32_t) + sizeof(double)) + sizeof(uint16_t));
 }
 
 template <int CS, int WK, int PREC, int VER>
@@ -1020,7 +1125,7 @@ void launch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, c
     using V = typename ValT<WK>::type;
     auto hash_launch = [&](auto kern, int slots, int gpb, int block, int bin, cudaStream_t str) {
         if (B.size[bin] == 0) return;
-        size_t smem = (size_t)slots * gpb * (sizeof(uint32_t) + sizeof(V));
+        size_t smem = (size_t)slots * gpb * (sizeof(uint32_t) + sizeof(V) + sizeof(uint16_t) / 2);
         MG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(B.size[bin], gpb), 148ull * 64);
         kern<<<grid, block, smem, str>>>(A, B.offset[bin], B.size[bin]);

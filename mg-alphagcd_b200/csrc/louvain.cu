@@ -44,6 +44,7 @@ struct Timer {
 // of the neighbour), 24 per vertex (offset, community, k_i, sigma of the own
 // community, new community), 8 per distinct candidate (sigma of the candidate).
 void account_sweep(mg_ctx *ctx, const GraphView &g, const SweepAcc &acc, mg_summary &S) {
+    MG_CHECK(acc.overflow == 0, MG_ERR_UNSUPPORTED, "local move: a cluster hash segment overflowed");
     float ms = 0;
     MG_CUDA(cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]));
     S.seconds_sweep_kernels += ms * 1e-3;

@@ -134,27 +134,39 @@ __global__ void __launch_bounds__(kRsThreads) rs_hist_kernel(const uint64_t *key
     hist[(size_t)threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
 }
 
+// Stable scatter of one tile: keys are ranked inside the tile (warp
+// match_any + per-warp digit counters), staged in shared memory in digit
+// order, and written out as contiguous runs per digit (coalesced).
 template <class V>
 __global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const uint64_t *keys, const V *vals,
                                                                   uint64_t *okeys, V *ovals, size_t n, int shift,
                                                                   const uint32_t *offs, uint32_t tiles) {
+    constexpr bool HasV = !std::is_same<V, NoVal>::value;
+    extern __shared__ __align__(16) unsigned char rs_smem[];
+    uint64_t *sk = (uint64_t *)rs_smem;                       // kRsTile keys
+    V *sv = (V *)(rs_smem + sizeof(uint64_t) * kRsTile);      // kRsTile values
     __shared__ uint32_t cnt[kRsWarps][256];
+    __shared__ uint32_t tstart[256], gofs[256], wsum[kRsWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int d = threadIdx.x; d < kRsWarps * 256; d += kRsThreads) (&cnt[0][0])[d] = 0;
     __syncthreads();
-    const size_t base = (size_t)blockIdx.x * kRsTile + (size_t)warp * (kRsRounds * 32);
+    const size_t tile0 = (size_t)blockIdx.x * kRsTile;
+    const uint32_t tile_n = (uint32_t)(n - tile0 < (size_t)kRsTile ? n - tile0 : (size_t)kRsTile);
+    const uint32_t wbase = (uint32_t)warp * (kRsRounds * 32);
     const uint32_t lt = (1u << lane) - 1u;
     uint64_t k[kRsRounds];
     uint32_t rank[kRsRounds];
+    V v[HasV ? kRsRounds : 1];
 #pragma unroll
     for (int r = 0; r < kRsRounds; r++) {
-        size_t i = base + (size_t)r * 32 + lane;
-        k[r] = i < n ? keys[i] : 0;
+        uint32_t li = wbase + r * 32 + lane;
+        k[r] = li < tile_n ? keys[tile0 + li] : 0;
+        if constexpr (HasV) v[r] = li < tile_n ? vals[tile0 + li] : V();
     }
 #pragma unroll
     for (int r = 0; r < kRsRounds; r++) {
-        size_t i = base + (size_t)r * 32 + lane;
-        uint32_t d = i < n ? (uint32_t)((k[r] >> shift) & 0xFF) : 0x100u;
+        uint32_t li = wbase + r * 32 + lane;
+        uint32_t d = li < tile_n ? (uint32_t)((k[r] >> shift) & 0xFF) : 0x100u;
         uint32_t peers = __match_any_sync(0xffffffffu, d);
         uint32_t before = __popc(peers & lt);
         uint32_t run = d < 256 ? cnt[warp][d] : 0;
@@ -164,27 +176,48 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const uint64_t *
         __syncwarp();
     }
     __syncthreads();
-    // exclusive prefix over warps per digit, plus the tile's global offset
     {
+        // per digit: exclusive prefix over warps, digit total, tile-wide
+        // exclusive scan of the totals, global offset of this tile's run
         const int d = threadIdx.x;
-        uint32_t acc = offs[(size_t)d * tiles + blockIdx.x];
+        uint32_t acc = 0;
 #pragma unroll
         for (int w = 0; w < kRsWarps; w++) {
             uint32_t c = cnt[w][d];
             cnt[w][d] = acc;
             acc += c;
         }
+        uint32_t incl = acc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        gofs[d] = offs[(size_t)d * tiles + blockIdx.x];
+        __syncthreads();
+        uint32_t before = 0;
+        for (int w = 0; w < warp; w++) before += wsum[w];
+        tstart[d] = before + incl - acc;
     }
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < kRsRounds; r++) {
-        size_t i = base + (size_t)r * 32 + lane;
-        if (i < n) {
+        uint32_t li = wbase + r * 32 + lane;
+        if (li < tile_n) {
             uint32_t d = (uint32_t)((k[r] >> shift) & 0xFF);
-            uint32_t pos = cnt[warp][d] + rank[r];
-            okeys[pos] = k[r];
-            if constexpr (!std::is_same<V, NoVal>::value) ovals[pos] = vals[i];
+            uint32_t pos = tstart[d] + cnt[warp][d] + rank[r];
+            sk[pos] = k[r];
+            if constexpr (HasV) sv[pos] = v[r];
         }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < tile_n; i += kRsThreads) {
+        const uint64_t key = sk[i];
+        const uint32_t d = (uint32_t)((key >> shift) & 0xFF);
+        const uint32_t pos = gofs[d] + (i - tstart[d]);
+        okeys[pos] = key;
+        if constexpr (HasV) ovals[pos] = sv[i];
     }
 }
 
@@ -200,11 +233,13 @@ bool radix_sort(uint64_t *keys, V *vals, uint64_t *keys_alt, V *vals_alt, size_t
     uint64_t *ka = keys, *kb = keys_alt;
     V *va = vals, *vb = vals_alt;
     bool flipped = false;
+    const size_t smem = (size_t)kRsTile * (sizeof(uint64_t) + (std::is_same<V, NoVal>::value ? 0 : sizeof(V)));
+    MG_CUDA(cudaFuncSetAttribute(rs_scatter_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     for (int shift = 0; shift < bits; shift += 8) {
         rs_hist_kernel<<<tiles, kRsThreads, 0, s>>>(ka, n, shift, hist, tiles);
         MG_LAUNCH_CHECK();
         exclusive_scan<uint32_t>(hist, hist, (size_t)tiles * 256, nullptr, s, ws);
-        rs_scatter_kernel<V><<<tiles, kRsThreads, 0, s>>>(ka, va, kb, vb, n, shift, hist, tiles);
+        rs_scatter_kernel<V><<<tiles, kRsThreads, smem, s>>>(ka, va, kb, vb, n, shift, hist, tiles);
         MG_LAUNCH_CHECK();
         std::swap(ka, kb);
         std::swap(va, vb);
