@@ -196,6 +196,71 @@ mg_status mg_result_level_sizes(const mg_result *r, uint32_t *out, int max, int 
 mg_status mg_result_trace(const mg_result *r, double *rows4, int max_rows, int *count);
 mg_status mg_result_destroy(mg_result *r);
 
+/* ---- batched form --------------------------------------------------------------
+ * No reference counterpart: the reference runs one graph per process.  A batch
+ * packs many independent graphs as one disjoint union on the device and runs
+ * louvain::run's control flow (src/louvain/louvain.cu:1401-1715) for every
+ * graph at once: one set of kernel launches per sweep covers all graphs, each
+ * graph keeps its own mass, gain constants, modularity, accept / reject
+ * decisions and phase exit, so each result is the one mg_louvain_run gives
+ * for that graph alone (bit for bit on integral weights). */
+typedef struct mg_batch mg_batch;
+typedef struct mg_batch_result mg_batch_result;
+
+/* parameters of one seeded SBM graph (mg_graph_generate_sbm) */
+typedef struct {
+    uint32_t n;
+    uint32_t blocks;
+    double mean_degree;
+    double intra_frac;
+    uint64_t seed;
+} mg_sbm_params;
+
+/* Draw per-graph SBM parameters on the host: n log-uniform in [n_min, n_max],
+ * blocks uniform in [blocks_min, min(blocks_max, n)], mean degree uniform in
+ * [deg_min, deg_max], intra-community fraction uniform in [intra_min,
+ * intra_max], graph seeds derived from seed.  Deterministic in seed. */
+mg_status mg_batch_draw_sbm_params(uint32_t graphs, uint32_t n_min, uint32_t n_max, uint32_t blocks_min,
+                                   uint32_t blocks_max, double deg_min, double deg_max, double intra_min,
+                                   double intra_max, uint64_t seed, mg_sbm_params *out);
+/* Generate graph g of the batch exactly as mg_graph_generate_sbm(params[g]). */
+mg_status mg_batch_generate_sbm(mg_ctx *ctx, uint32_t graphs, const mg_sbm_params *params, mg_batch **out);
+/* Pack host graphs: graph g owns vertices [vertex_offsets[g], vertex_offsets[g+1])
+ * of the packed rows; row v's entries are [offsets[v], offsets[v+1]) (64-bit,
+ * packed over all graphs); cols hold graph-local vertex ids.  weights as in
+ * mg_graph_from_csr (NULL = unit). */
+mg_status mg_batch_from_csr(mg_ctx *ctx, uint32_t graphs, const uint64_t *vertex_offsets, const uint64_t *offsets,
+                            const uint32_t *cols, const void *weights, int weight_type, mg_batch **out);
+/* total vertices / entries of the batch */
+mg_status mg_batch_info(const mg_batch *b, uint32_t *graphs, uint64_t *n, uint64_t *nnz);
+/* one graph: vertices, entries, mass */
+mg_status mg_batch_graph_info(const mg_batch *b, uint32_t g, uint32_t *n, uint64_t *nnz, double *mass);
+mg_status mg_batch_destroy(mg_batch *b);
+
+enum {
+    MG_BATCH_GRAPHS = 1 /* run each phase's iterations as one CUDA graph with a device-side loop */
+};
+
+typedef struct {
+    double modularity;
+    uint32_t n;
+    uint64_t nnz;
+    int phases;
+    int levels;
+    uint64_t iterations;
+    uint32_t communities;
+} mg_batch_graph_summary;
+
+/* Run Louvain on every graph of the batch.  flags: MG_BATCH_*. */
+mg_status mg_batch_run(mg_batch *b, const mg_run_opts *opts /* may be NULL */, int flags, mg_batch_result **out);
+/* totals of the run (seconds, sweeps, edges, launches); per-graph fields
+ * (modularity, phases, levels, iterations, communities) are left zero */
+mg_status mg_batch_result_summary(const mg_batch_result *r, mg_summary *s);
+mg_status mg_batch_result_graph(const mg_batch_result *r, uint32_t g, mg_batch_graph_summary *out);
+/* final community (dense, graph-local) of every vertex of graph g: n_g entries */
+mg_status mg_batch_result_assignment(const mg_batch_result *r, uint32_t g, uint32_t *out);
+mg_status mg_batch_result_destroy(mg_batch_result *r);
+
 #ifdef __cplusplus
 }
 #endif

@@ -15,6 +15,8 @@ Interfaces mirror the reference's stage boundaries (MG-alphaGCD):
   Graph.modularity        -> compute_modularity         (src/louvain/louvain.cu:105-238)
   Graph.coarsen           -> coarsen_graph_mg::coarsen_graph (src/coarsen_graph/coarsen_graph_mg.cu:2054)
   Graph.louvain           -> louvain::run               (src/louvain/louvain.cu:1401)
+  Batch.run               -> louvain::run for every graph of a packed batch (no reference
+                             counterpart: the reference runs one graph per process)
 """
 from __future__ import annotations
 
@@ -61,12 +63,27 @@ class _Summary(ct.Structure):
                 ("kernel_launches", ct.c_uint64), ("sweeps", ct.c_uint64)]
 
 
+class SbmParams(ct.Structure):
+    _fields_ = [("n", ct.c_uint32), ("blocks", ct.c_uint32), ("mean_degree", ct.c_double),
+                ("intra_frac", ct.c_double), ("seed", ct.c_uint64)]
+
+
+class _BatchGraph(ct.Structure):
+    _fields_ = [("modularity", ct.c_double), ("n", ct.c_uint32), ("nnz", ct.c_uint64), ("phases", ct.c_int),
+                ("levels", ct.c_int), ("iterations", ct.c_uint64), ("communities", ct.c_uint32)]
+
+
+BATCH_GRAPHS = 1
+
 EXPORTED = [
     "mg_status_string", "mg_version", "mg_init", "mg_destroy", "mg_last_error", "mg_graph_from_csr",
     "mg_graph_from_device_csr", "mg_graph_from_mtx", "mg_graph_generate_rmat", "mg_graph_generate_sbm",
     "mg_graph_info", "mg_graph_copy_csr", "mg_graph_destroy", "mg_bins", "mg_bins_offsets", "mg_local_move",
     "mg_modularity", "mg_coarsen", "mg_louvain_run", "mg_result_summary", "mg_result_assignment",
-    "mg_result_level_sizes", "mg_result_trace", "mg_result_destroy",
+    "mg_result_level_sizes", "mg_result_trace", "mg_result_destroy", "mg_local_move_noalloc",
+    "mg_batch_draw_sbm_params", "mg_batch_generate_sbm", "mg_batch_from_csr", "mg_batch_info",
+    "mg_batch_graph_info", "mg_batch_destroy", "mg_batch_run", "mg_batch_result_summary", "mg_batch_result_graph",
+    "mg_batch_result_assignment", "mg_batch_result_destroy",
 ]
 
 
@@ -107,6 +124,17 @@ def lib():
     L.mg_result_level_sizes.argtypes = [vp, vp, i32, ct.POINTER(i32)]
     L.mg_result_trace.argtypes = [vp, vp, i32, ct.POINTER(i32)]
     L.mg_result_destroy.argtypes = [vp]
+    L.mg_batch_draw_sbm_params.argtypes = [u32, u32, u32, u32, u32, dbl, dbl, dbl, dbl, u64, vp]
+    L.mg_batch_generate_sbm.argtypes = [vp, u32, vp, pp]
+    L.mg_batch_from_csr.argtypes = [vp, u32, vp, vp, vp, vp, i32, pp]
+    L.mg_batch_info.argtypes = [vp, ct.POINTER(u32), ct.POINTER(u64), ct.POINTER(u64)]
+    L.mg_batch_graph_info.argtypes = [vp, u32, ct.POINTER(u32), ct.POINTER(u64), ct.POINTER(dbl)]
+    L.mg_batch_destroy.argtypes = [vp]
+    L.mg_batch_run.argtypes = [vp, ct.POINTER(_RunOpts), i32, pp]
+    L.mg_batch_result_summary.argtypes = [vp, ct.POINTER(_Summary)]
+    L.mg_batch_result_graph.argtypes = [vp, u32, ct.POINTER(_BatchGraph)]
+    L.mg_batch_result_assignment.argtypes = [vp, u32, vp]
+    L.mg_batch_result_destroy.argtypes = [vp]
     _lib = L
     return L
 
@@ -190,6 +218,118 @@ class Context:
                    "mg_bins_offsets")
         nb = {0: 10, 1: 11, 2: 9}[scheme]
         return {"sizes": sizes[:nb], "offsets": boff[:nb], "perm": perm[:n], "max_degree": int(md.value)}
+
+
+    # ---- batches ------------------------------------------------------------
+    def batch_generate_sbm(self, params) -> "Batch":
+        """Batch of seeded SBMs; graph g equals generate_sbm(**params[g])."""
+        arr = (SbmParams * len(params))(*[p if isinstance(p, SbmParams) else SbmParams(
+            p["n"], p["blocks"], p["mean_degree"], p["intra_frac"], p["seed"]) for p in params])
+        h = ct.c_void_p()
+        self.check(lib().mg_batch_generate_sbm(self.h, len(params), ct.cast(arr, ct.c_void_p), ct.byref(h)),
+                   "mg_batch_generate_sbm")
+        return Batch(self, h)
+
+    def batch_from_csr(self, graphs) -> "Batch":
+        """Pack host graphs [(n, offsets, cols, weights|None), ...] (local ids)."""
+        G = len(graphs)
+        voff = np.zeros(G + 1, np.uint64)
+        for g, (n, _, _, _) in enumerate(graphs):
+            voff[g + 1] = voff[g] + n
+        total = int(voff[-1])
+        off = np.zeros(total + 1, np.uint64)
+        cols, ws = [], []
+        base = 0
+        weighted = any(w is not None for _, _, _, w in graphs)
+        f32 = weighted and all(w is None or np.asarray(w).dtype == np.float32 for _, _, _, w in graphs)
+        for g, (n, o, c, w) in enumerate(graphs):
+            o = np.asarray(o, np.uint64)
+            off[int(voff[g]) + 1: int(voff[g]) + n + 1] = o[1:] + base
+            cols.append(np.asarray(c, np.uint32))
+            if weighted:
+                ws.append(np.ones(len(c)) if w is None else np.asarray(w, np.float64))
+            base += int(o[-1])
+        col = np.ascontiguousarray(np.concatenate(cols) if cols else np.zeros(0, np.uint32), dtype=np.uint32)
+        if weighted:
+            wt = WEIGHT_F32 if f32 else WEIGHT_F64
+            w = np.ascontiguousarray(np.concatenate(ws), dtype=np.float32 if f32 else np.float64)
+        else:
+            wt, w = WEIGHT_UNIT, None
+        h = ct.c_void_p()
+        self.check(lib().mg_batch_from_csr(self.h, G, _p(voff), _p(off), _p(col), _p(w), wt, ct.byref(h)),
+                   "mg_batch_from_csr")
+        return Batch(self, h)
+
+
+def draw_sbm_params(graphs: int, n_range=(1000, 200000), blocks_range=(4, 256), deg_range=(8.0, 32.0),
+                    intra_range=(0.7, 0.9), seed: int = 4) -> list:
+    """Per-graph SBM parameters of a batch (mg_batch_draw_sbm_params)."""
+    arr = (SbmParams * max(graphs, 1))()
+    st = lib().mg_batch_draw_sbm_params(graphs, n_range[0], n_range[1], blocks_range[0], blocks_range[1],
+                                        deg_range[0], deg_range[1], intra_range[0], intra_range[1], seed,
+                                        ct.cast(arr, ct.c_void_p))
+    if st != MG_OK:
+        raise MGError(st, lib().mg_last_error(None).decode())
+    return [{"n": p.n, "blocks": p.blocks, "mean_degree": p.mean_degree, "intra_frac": p.intra_frac,
+             "seed": p.seed} for p in arr[:graphs]]
+
+
+class Batch:
+    """Many graphs packed on the device (mg_batch)."""
+
+    def __init__(self, ctx: Context, h: ct.c_void_p):
+        self.ctx = ctx
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().mg_batch_destroy(self.h)
+            self.h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        g, n, nnz = ct.c_uint32(), ct.c_uint64(), ct.c_uint64()
+        self.ctx.check(lib().mg_batch_info(self.h, ct.byref(g), ct.byref(n), ct.byref(nnz)), "mg_batch_info")
+        return {"graphs": g.value, "n": n.value, "nnz": nnz.value}
+
+    def graph_info(self, g: int) -> dict:
+        n, nnz, mass = ct.c_uint32(), ct.c_uint64(), ct.c_double()
+        self.ctx.check(lib().mg_batch_graph_info(self.h, g, ct.byref(n), ct.byref(nnz), ct.byref(mass)),
+                       "mg_batch_graph_info")
+        return {"n": n.value, "nnz": nnz.value, "mass": mass.value}
+
+    def run(self, version: int = 2, threshold: float = 1e-6, max_phases: int = 1000, precision: str = "fp64",
+            graphs: bool = True, assignments: bool = True) -> dict:
+        opts = _RunOpts(version, threshold, max_phases, _PREC[precision], 0)
+        r = ct.c_void_p()
+        self.ctx.check(lib().mg_batch_run(self.h, ct.byref(opts), BATCH_GRAPHS if graphs else 0, ct.byref(r)),
+                       "mg_batch_run")
+        try:
+            s = _Summary()
+            lib().mg_batch_result_summary(r, ct.byref(s))
+            out = {f: getattr(s, f) for f, _ in _Summary._fields_}
+            G = self.info()["graphs"]
+            per = {f: [] for f, _ in _BatchGraph._fields_}
+            assign = []
+            bg = _BatchGraph()
+            for g in range(G):
+                lib().mg_batch_result_graph(r, g, ct.byref(bg))
+                for f, _ in _BatchGraph._fields_:
+                    per[f].append(getattr(bg, f))
+                if assignments:
+                    a = np.zeros(max(bg.n, 1), np.uint32)
+                    lib().mg_batch_result_assignment(r, g, _p(a))
+                    assign.append(a[: bg.n])
+            out["graphs"] = {f: np.array(v) for f, v in per.items()}
+            out["assignments"] = assign
+            return out
+        finally:
+            lib().mg_batch_result_destroy(r)
 
 
 class Graph:

@@ -1,6 +1,7 @@
 // capi.cu -- the extern "C" entry points declared in include/mgagcd.h.
 // Every entry point catches engine errors and returns an mg_status; the
 // message of the last failure is kept on the context.
+#include <cmath>
 #include <cstring>
 #include <new>
 
@@ -471,6 +472,147 @@ mg_status mg_result_trace(const mg_result *r, double *rows4, int max_rows, int *
 }
 
 mg_status mg_result_destroy(mg_result *r) {
+    if (!r) return MG_ERR_INVALID;
+    delete r;
+    return MG_OK;
+}
+
+// ---- batched form -------------------------------------------------------------
+
+mg_status mg_batch_draw_sbm_params(uint32_t graphs, uint32_t n_min, uint32_t n_max, uint32_t blocks_min,
+                                   uint32_t blocks_max, double deg_min, double deg_max, double intra_min,
+                                   double intra_max, uint64_t seed, mg_sbm_params *out) {
+    if (!out && graphs) return fail(nullptr, MG_ERR_INVALID, "mg_batch_draw_sbm_params: out is NULL");
+    if (n_min < 1 || n_max < n_min || blocks_min < 1 || blocks_max < blocks_min || deg_max < deg_min ||
+        intra_max < intra_min || intra_min < 0 || intra_max > 1)
+        return fail(nullptr, MG_ERR_INVALID, "mg_batch_draw_sbm_params: bad ranges");
+    const uint64_t key = rng_key(seed, 0x42415443ull);
+    auto unif = [&](uint64_t ctr) { return (double)(rng_at(key, ctr) >> 11) * (1.0 / 9007199254740992.0); };
+    const double l0 = std::log((double)n_min), l1 = std::log((double)n_max);
+    for (uint32_t g = 0; g < graphs; g++) {
+        mg_sbm_params &p = out[g];
+        double nv = std::floor(std::exp(l0 + unif(5ull * g) * (l1 - l0)) + 0.5);
+        nv = nv < n_min ? n_min : nv > n_max ? n_max : nv;
+        p.n = (uint32_t)nv;
+        const uint32_t bmax = blocks_max < p.n ? blocks_max : p.n;
+        const uint32_t bmin = blocks_min < bmax ? blocks_min : bmax;
+        p.blocks = bmin + (uint32_t)(unif(5ull * g + 1) * (double)(bmax - bmin + 1));
+        if (p.blocks > bmax) p.blocks = bmax;
+        p.mean_degree = deg_min + unif(5ull * g + 2) * (deg_max - deg_min);
+        p.intra_frac = intra_min + unif(5ull * g + 3) * (intra_max - intra_min);
+        p.seed = rng_at(key, 5ull * g + 4);
+    }
+    return MG_OK;
+}
+
+static mg_status batch_new(mg_ctx *ctx, uint32_t graphs, mg_batch **out, mg_batch **b) {
+    if (!ctx || !out) return fail(ctx, MG_ERR_INVALID, "batch: NULL argument");
+    *out = nullptr;
+    if (graphs < 1) return fail(ctx, MG_ERR_INVALID, "batch: need at least one graph");
+    *b = new (std::nothrow) mg_batch();
+    if (!*b) return fail(ctx, MG_ERR_OOM, "host allocation failed");
+    (*b)->ctx = ctx;
+    (*b)->u.ctx = ctx;
+    (*b)->graphs = graphs;
+    return MG_OK;
+}
+
+mg_status mg_batch_generate_sbm(mg_ctx *ctx, uint32_t graphs, const mg_sbm_params *params, mg_batch **out) {
+    mg_batch *b = nullptr;
+    mg_status st = batch_new(ctx, graphs, out, &b);
+    if (st != MG_OK) return st;
+    st = guarded(ctx, [&] { batch_generate_sbm(b, params); });
+    if (st != MG_OK) {
+        delete b;
+        return st;
+    }
+    *out = b;
+    return MG_OK;
+}
+
+mg_status mg_batch_from_csr(mg_ctx *ctx, uint32_t graphs, const uint64_t *vertex_offsets, const uint64_t *offsets,
+                            const uint32_t *cols, const void *weights, int weight_type, mg_batch **out) {
+    mg_batch *b = nullptr;
+    mg_status st = batch_new(ctx, graphs, out, &b);
+    if (st != MG_OK) return st;
+    st = guarded(ctx, [&] { batch_from_host_csr(b, vertex_offsets, offsets, cols, weights, weight_type); });
+    if (st != MG_OK) {
+        delete b;
+        return st;
+    }
+    *out = b;
+    return MG_OK;
+}
+
+mg_status mg_batch_info(const mg_batch *b, uint32_t *graphs, uint64_t *n, uint64_t *nnz) {
+    if (!b) return MG_ERR_INVALID;
+    if (graphs) *graphs = b->graphs;
+    if (n) *n = b->u.n;
+    if (nnz) *nnz = b->u.nnz;
+    return MG_OK;
+}
+
+mg_status mg_batch_graph_info(const mg_batch *b, uint32_t g, uint32_t *n, uint64_t *nnz, double *mass) {
+    if (!b) return MG_ERR_INVALID;
+    if (g >= b->graphs) return fail(b->ctx, MG_ERR_INVALID, "batch: graph index out of range");
+    if (n) *n = b->voff[g + 1] - b->voff[g];
+    if (nnz) *nnz = b->eoff[g + 1] - b->eoff[g];
+    if (mass) *mass = b->mass[g];
+    return MG_OK;
+}
+
+mg_status mg_batch_destroy(mg_batch *b) {
+    if (!b) return MG_ERR_INVALID;
+    cudaSetDevice(b->ctx->device);
+    delete b;
+    return MG_OK;
+}
+
+mg_status mg_batch_run(mg_batch *b, const mg_run_opts *opts, int flags, mg_batch_result **out) {
+    if (!b || !out) return MG_ERR_INVALID;
+    *out = nullptr;
+    mg_ctx *ctx = b->ctx;
+    mg_run_opts o;
+    o.version = 2;
+    o.threshold = 1e-6;
+    o.max_phases = 1000;
+    o.precision = MG_PREC_FP64;
+    o.verbose = 0;
+    if (opts) o = *opts;
+    if (o.version < 0 || o.version > 2) return fail(ctx, MG_ERR_INVALID, "version must be 0, 1 or 2");
+    if (o.precision < 0 || o.precision > 2) return fail(ctx, MG_ERR_INVALID, "unknown precision");
+    if (flags & ~MG_BATCH_GRAPHS) return fail(ctx, MG_ERR_INVALID, "unknown batch flags");
+    mg_batch_result *r = new (std::nothrow) mg_batch_result();
+    if (!r) return fail(ctx, MG_ERR_OOM, "host allocation failed");
+    mg_status st = guarded(ctx, [&] { batch_run(b, o, flags, *r); });
+    if (st != MG_OK) {
+        delete r;
+        return st;
+    }
+    *out = r;
+    return MG_OK;
+}
+
+mg_status mg_batch_result_summary(const mg_batch_result *r, mg_summary *s) {
+    if (!r || !s) return MG_ERR_INVALID;
+    *s = r->sum;
+    return MG_OK;
+}
+
+mg_status mg_batch_result_graph(const mg_batch_result *r, uint32_t g, mg_batch_graph_summary *out) {
+    if (!r || !out || g >= r->graphs) return MG_ERR_INVALID;
+    *out = r->per[g];
+    return MG_OK;
+}
+
+mg_status mg_batch_result_assignment(const mg_batch_result *r, uint32_t g, uint32_t *out) {
+    if (!r || !out || g >= r->graphs) return MG_ERR_INVALID;
+    const uint32_t n = r->voff[g + 1] - r->voff[g];
+    if (n) memcpy(out, r->assignment.data() + r->voff[g], sizeof(uint32_t) * n);
+    return MG_OK;
+}
+
+mg_status mg_batch_result_destroy(mg_batch_result *r) {
     if (!r) return MG_ERR_INVALID;
     delete r;
     return MG_OK;

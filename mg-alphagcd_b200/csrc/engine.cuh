@@ -96,12 +96,58 @@ struct SweepParams {
     int integral = 0;
 };
 
+// Constants of the gain of one graph, from its mass (sum of all directed
+// weights): m = mass/2 and the correctly rounded reciprocals the exact
+// division by m and 2m uses, in FP64 and FP32, and the mass as an integer.
+struct GainK {
+    double m, two_m, r_m, r_two_m;
+    float m_f, two_m_f, r_m_f, r_two_m_f;
+    long long mass_i;
+};
+GainK gain_constants(double mass);
+
+// Batched sweeps run the local move of many graphs packed as one disjoint
+// union.  Each graph has a control word:
+//   bit 0      active: its vertices take part in the next sweep
+//   bits 1-2   assignment buffer the sweep reads (P)
+//   bits 3-4   assignment buffer the sweep writes (N)
+//   bits 5-6   buffer holding the last accepted assignment (base)
+//   bit 7      the next sweep is the first of the phase
+//   bit 8      a sigma update is pending
+//   bits 9-10  / 11-12  the update moves vertices from buffer / to buffer
+constexpr uint32_t kGwActive = 1u, kGwFirst = 1u << 7, kGwUpdate = 1u << 8;
+__host__ __device__ inline uint32_t gw_p(uint32_t w) { return (w >> 1) & 3u; }
+__host__ __device__ inline uint32_t gw_n(uint32_t w) { return (w >> 3) & 3u; }
+__host__ __device__ inline uint32_t gw_base(uint32_t w) { return (w >> 5) & 3u; }
+__host__ __device__ inline uint32_t gw_from(uint32_t w) { return (w >> 9) & 3u; }
+__host__ __device__ inline uint32_t gw_to(uint32_t w) { return (w >> 11) & 3u; }
+__host__ __device__ inline uint32_t gw_make(bool active, uint32_t p, uint32_t n, uint32_t base, bool first,
+                                            bool update, uint32_t from, uint32_t to) {
+    return (active ? kGwActive : 0u) | (p << 1) | (n << 3) | (base << 5) | (first ? kGwFirst : 0u) |
+           (update ? kGwUpdate : 0u) | (from << 9) | (to << 11);
+}
+
+struct BatchSweep {
+    const uint32_t *perm = nullptr;   // bins 0-8 list (the level's bins give its sizes)
+    const uint32_t *pgid = nullptr;   // graph of each entry of perm
+    const uint32_t *gid = nullptr;    // graph of each vertex of the union
+    const uint32_t *gword = nullptr;  // control word per graph
+    const GainK *gk = nullptr;        // gain constants per graph
+    uint32_t *C[3] = {nullptr, nullptr, nullptr};
+    double *sinv = nullptr;           // out: sum_in contribution per vertex
+    const int *up = nullptr;          // sweep direction (device)
+};
+
 // Prepare a level: bins (scheme 0) and heavy-vertex tables.
 void move_prepare_level(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, cudaStream_t s);
 // One local-move sweep P -> N (plus the internal-weight sum of P), device
 // accumulators in ws.acc (zeroed by the caller via sweep_reset_acc).
 void move_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p,
                 const uint32_t *P, uint32_t *N, const double *k, const double *sigma, cudaStream_t s);
+// The same sweep over a batch: per vertex, the graph's control word selects
+// the buffers and the gain constants, and sum_in goes to b.sinv.
+void move_sweep_batch(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p,
+                      const BatchSweep &b, const double *k, const double *sigma, cudaStream_t s);
 void sweep_reset_acc(MoveWorkspace &ws, cudaStream_t s);
 // sum of sigma^2 into ws.acc
 void sigma_sumsq(const double *sigma, uint32_t n, int integral, MoveWorkspace &ws, cudaStream_t s);

@@ -35,27 +35,91 @@ __global__ void rmat_pairs_kernel(int scale, uint64_t m, uint64_t t1, uint64_t t
     }
 }
 
+// pair k of a seeded SBM: the first min_ pairs join two vertices of one block,
+// the rest two vertices of different blocks (block b holds [b*n/blocks,
+// (b+1)*n/blocks))
+__device__ __forceinline__ void sbm_pair(uint32_t n, uint32_t blocks, uint64_t min_, uint64_t kin, uint64_t kout,
+                                         uint64_t k, uint32_t &u, uint32_t &v) {
+    if (k < min_) {
+        uint64_t r0 = rng_at(kin, 2 * k), r1 = rng_at(kin, 2 * k + 1);
+        uint32_t bb = uni32((uint32_t)r0, blocks);
+        uint32_t lo = (uint32_t)((uint64_t)bb * n / blocks), hi = (uint32_t)((uint64_t)(bb + 1) * n / blocks);
+        u = lo + uni32((uint32_t)(r0 >> 32), hi - lo);
+        v = lo + uni32((uint32_t)r1, hi - lo);
+    } else {
+        uint64_t j = k - min_;
+        uint64_t r0 = rng_at(kout, 2 * j), r1 = rng_at(kout, 2 * j + 1);
+        uint32_t b1 = uni32((uint32_t)r0, blocks);
+        uint32_t b2 = uni32((uint32_t)(r0 >> 32), blocks - 1);
+        if (b2 >= b1) b2++;
+        uint32_t lo1 = (uint32_t)((uint64_t)b1 * n / blocks), hi1 = (uint32_t)((uint64_t)(b1 + 1) * n / blocks);
+        uint32_t lo2 = (uint32_t)((uint64_t)b2 * n / blocks), hi2 = (uint32_t)((uint64_t)(b2 + 1) * n / blocks);
+        u = lo1 + uni32((uint32_t)r1, hi1 - lo1);
+        v = lo2 + uni32((uint32_t)(r1 >> 32), hi2 - lo2);
+    }
+}
+
 __global__ void sbm_pairs_kernel(uint32_t n, uint32_t blocks, uint64_t min_, uint64_t m, uint64_t kin, uint64_t kout,
                                  uint32_t *u, uint32_t *v) {
-    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (uint64_t)gridDim.x * blockDim.x) {
-        if (k < min_) {
-            uint64_t r0 = rng_at(kin, 2 * k), r1 = rng_at(kin, 2 * k + 1);
-            uint32_t bb = uni32((uint32_t)r0, blocks);
-            uint32_t lo = (uint32_t)((uint64_t)bb * n / blocks), hi = (uint32_t)((uint64_t)(bb + 1) * n / blocks);
-            u[k] = lo + uni32((uint32_t)(r0 >> 32), hi - lo);
-            v[k] = lo + uni32((uint32_t)r1, hi - lo);
-        } else {
-            uint64_t j = k - min_;
-            uint64_t r0 = rng_at(kout, 2 * j), r1 = rng_at(kout, 2 * j + 1);
-            uint32_t b1 = uni32((uint32_t)r0, blocks);
-            uint32_t b2 = uni32((uint32_t)(r0 >> 32), blocks - 1);
-            if (b2 >= b1) b2++;
-            uint32_t lo1 = (uint32_t)((uint64_t)b1 * n / blocks), hi1 = (uint32_t)((uint64_t)(b1 + 1) * n / blocks);
-            uint32_t lo2 = (uint32_t)((uint64_t)b2 * n / blocks), hi2 = (uint32_t)((uint64_t)(b2 + 1) * n / blocks);
-            u[k] = lo1 + uni32((uint32_t)r1, hi1 - lo1);
-            v[k] = lo2 + uni32((uint32_t)(r1 >> 32), hi2 - lo2);
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (uint64_t)gridDim.x * blockDim.x)
+        sbm_pair(n, blocks, min_, kin, kout, k, u[k], v[k]);
+}
+
+// per-graph parameters of a batch of SBMs
+struct SbmDev {
+    uint32_t n, blocks, vbase, pad;
+    uint64_t min_, kin, kout, pbase;  // pbase: first pair of the graph
+};
+
+// all pairs of all graphs of a batch; graph of pair k by binary search over
+// the pair bases (G + 1 entries)
+__global__ void sbm_batch_pairs_kernel(const SbmDev *gp, const uint64_t *pbase, uint32_t G, uint64_t M, uint32_t *u,
+                                       uint32_t *v) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M; k += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = G;  // last graph with pbase <= k
+        while (hi - lo > 1) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (pbase[mid] <= k) lo = mid;
+            else hi = mid;
+        }
+        const SbmDev p = gp[lo];
+        uint32_t a, b;
+        sbm_pair(p.n, p.blocks, p.min_, p.kin, p.kout, k - p.pbase, a, b);
+        u[k] = p.vbase + a;
+        v[k] = p.vbase + b;
+    }
+}
+
+// packed rows of a batch from the host: 64-bit row offsets -> 32-bit, local
+// column ids -> union ids; flags non-monotone offsets (bit 0) and column ids
+// outside the row's graph (bit 1).  One warp per row.
+__global__ void batch_rows_kernel(const uint64_t *off64, uint32_t n, const uint32_t *voff, uint32_t G, uint32_t *cols,
+                                  uint32_t *off32, int *bad) {
+    const uint32_t lane = threadIdx.x & 31;
+    int b = 0;
+    for (uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v <= n;
+         v += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
+        const uint64_t o = off64[v];
+        if (lane == 0) {
+            off32[v] = (uint32_t)o;
+            if (v > 0 && o < off64[v - 1]) b |= 1;
+        }
+        if (v == n) continue;
+        uint32_t lo = 0, hi = G;  // graph of row v: last g with voff[g] <= v
+        while (hi - lo > 1) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (voff[mid] <= v) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t base = voff[lo], ng = voff[lo + 1] - base;
+        const uint64_t e1 = off64[v + 1];
+        for (uint64_t e = o + lane; e < e1; e += 32) {
+            const uint32_t c = cols[e];
+            if (c >= ng) b |= 2;
+            else cols[e] = base + c;
         }
     }
+    if (b) atomicOr(bad, b);
 }
 
 // 64-bit offsets -> 32-bit; flags non-monotone offsets (bit 0) and column ids
@@ -287,6 +351,175 @@ void graph_generate_sbm(mg_graph *g, uint32_t n, uint32_t blocks, double mean_de
         MG_LAUNCH_CHECK();
     }
     finish_generated(g, n, m, u, v);
+}
+
+// ---- batches -----------------------------------------------------------------
+
+namespace {
+__global__ void gather_u32_kernel(const uint32_t *src, const uint32_t *idx, uint32_t m, uint32_t *dst) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) dst[i] = src[idx[i]];
+}
+}  // namespace
+
+// entry offsets of the graphs of a packed union (offsets at the first vertex of
+// each graph)
+static void batch_entry_offsets(mg_batch *b) {
+    cudaStream_t s = b->ctx->stream;
+    const uint32_t G = b->graphs;
+    DBuf<uint32_t> idx, out;
+    MG_CUDA(cudaMemcpyAsync(idx.ensure(G + 1), b->voff.data(), sizeof(uint32_t) * (G + 1), cudaMemcpyHostToDevice, s));
+    gather_u32_kernel<<<(unsigned)ceil_div(G + 1, 256), 256, 0, s>>>(b->u.off.get(), idx.get(), G + 1,
+                                                                     out.ensure(G + 1));
+    MG_LAUNCH_CHECK();
+    std::vector<uint32_t> h(G + 1);
+    MG_CUDA(cudaMemcpyAsync(h.data(), out.get(), sizeof(uint32_t) * (G + 1), cudaMemcpyDeviceToHost, s));
+    MG_CUDA(cudaStreamSynchronize(s));
+    b->eoff.assign(h.begin(), h.end());
+}
+
+void batch_generate_sbm(mg_batch *b, const mg_sbm_params *params) {
+    const uint32_t G = b->graphs;
+    MG_CHECK(G >= 1 && params != nullptr, MG_ERR_INVALID, "batch: need at least one graph and its parameters");
+    std::vector<SbmDev> gp(G);
+    std::vector<uint64_t> pbase(G + 1, 0);
+    b->voff.assign(G + 1, 0);
+    uint64_t nv = 0, M = 0;
+    for (uint32_t g = 0; g < G; g++) {
+        const mg_sbm_params &p = params[g];
+        MG_CHECK(p.blocks >= 1 && p.n >= p.blocks, MG_ERR_INVALID, "sbm: need 1 <= blocks <= n");
+        // pair counts exactly as graph_generate_sbm
+        const double din = p.mean_degree * p.intra_frac;
+        const double dout = p.mean_degree - din;
+        const uint64_t min_ = (uint64_t)std::llround((double)p.n * din / 2.0);
+        const uint64_t mout = p.blocks > 1 ? (uint64_t)std::llround((double)p.n * dout / 2.0) : 0;
+        gp[g].n = p.n;
+        gp[g].blocks = p.blocks;
+        gp[g].vbase = (uint32_t)nv;
+        gp[g].min_ = min_;
+        gp[g].kin = rng_key(p.seed, 0x53424d31ull);
+        gp[g].kout = rng_key(p.seed, 0x53424d32ull);
+        gp[g].pbase = M;
+        pbase[g] = M;
+        b->voff[g] = (uint32_t)nv;
+        nv += p.n;
+        M += min_ + mout;
+        MG_CHECK(nv < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "batch: more than 2^32-1 vertices in total");
+        MG_CHECK(2 * M < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "batch: more than 2^32-1 directed entries in total");
+    }
+    pbase[G] = M;
+    b->voff[G] = (uint32_t)nv;
+    cudaStream_t s = b->ctx->stream;
+    DBuf<uint32_t> u, v;
+    u.ensure(M + 1);
+    v.ensure(M + 1);
+    if (M > 0) {
+        DBuf<SbmDev> dgp;
+        DBuf<uint64_t> dpb;
+        MG_CUDA(cudaMemcpyAsync(dgp.ensure(G), gp.data(), sizeof(SbmDev) * G, cudaMemcpyHostToDevice, s));
+        MG_CUDA(cudaMemcpyAsync(dpb.ensure(G + 1), pbase.data(), sizeof(uint64_t) * (G + 1), cudaMemcpyHostToDevice,
+                                s));
+        sbm_batch_pairs_kernel<<<148 * 16, 256, 0, s>>>(dgp.get(), dpb.get(), G, M, u.get(), v.get());
+        MG_LAUNCH_CHECK();
+        MG_CUDA(cudaStreamSynchronize(s));
+    }
+    finish_generated(&b->u, (uint32_t)nv, M, u, v);
+    batch_entry_offsets(b);
+    b->mass.resize(G);
+    b->integral.resize(G);
+    for (uint32_t g = 0; g < G; g++) {
+        b->mass[g] = (double)(b->eoff[g + 1] - b->eoff[g]);
+        b->integral[g] = 1;
+    }
+}
+
+void batch_from_host_csr(mg_batch *b, const uint64_t *voff, const uint64_t *offsets, const uint32_t *cols,
+                         const void *w, int weight_type) {
+    const uint32_t G = b->graphs;
+    MG_CHECK(G >= 1 && voff != nullptr && offsets != nullptr, MG_ERR_INVALID, "batch: NULL offsets");
+    MG_CHECK(voff[0] == 0, MG_ERR_INVALID, "batch: vertex_offsets[0] must be 0");
+    for (uint32_t g = 0; g < G; g++)
+        MG_CHECK(voff[g + 1] >= voff[g], MG_ERR_INVALID, "batch: vertex offsets must be non-decreasing");
+    const uint64_t n = voff[G];
+    MG_CHECK(n < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "batch: more than 2^32-1 vertices in total");
+    MG_CHECK(offsets[0] == 0, MG_ERR_INVALID, "offsets[0] must be 0");
+    const uint64_t nnz = offsets[n];
+    MG_CHECK(nnz < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "batch: more than 2^32-1 directed entries in total");
+    MG_CHECK(nnz == 0 || cols != nullptr, MG_ERR_INVALID, "cols is NULL");
+    MG_CHECK(weight_type >= MG_WEIGHT_UNIT && weight_type <= MG_WEIGHT_F64, MG_ERR_INVALID, "bad weight type");
+    MG_CHECK(weight_type == MG_WEIGHT_UNIT || nnz == 0 || w != nullptr, MG_ERR_INVALID, "weights is NULL");
+    b->voff.resize(G + 1);
+    b->eoff.resize(G + 1);
+    for (uint32_t g = 0; g <= G; g++) {
+        b->voff[g] = (uint32_t)voff[g];
+        b->eoff[g] = offsets[voff[g]];
+    }
+    for (uint32_t g = 0; g < G; g++)
+        MG_CHECK(b->eoff[g + 1] >= b->eoff[g], MG_ERR_INVALID, "offsets must be non-decreasing");
+    // mass of each graph in its CSR order (src/graph/host_graph.cpp:112-115),
+    // integrality, unit detection -- as graph_from_host_csr does per graph
+    b->mass.assign(G, 0.0);
+    b->integral.assign(G, 1);
+    bool unit = true;
+    for (uint32_t g = 0; g < G; g++) {
+        const uint64_t e0 = b->eoff[g], e1 = b->eoff[g + 1];
+        double mass = (double)(e1 - e0);
+        bool nonint = false;
+        if (weight_type != MG_WEIGHT_UNIT) {
+            mass = 0;
+            for (uint64_t e = e0; e < e1; e++) {
+                double x = weight_type == MG_WEIGHT_F32 ? (double)((const float *)w)[e] : ((const double *)w)[e];
+                mass += x;
+                nonint |= (x < 0 || x != std::floor(x));
+                unit &= (x == 1.0);
+            }
+        }
+        b->mass[g] = mass;
+        b->integral[g] = !nonint && mass < 4294967296.0;
+    }
+    mg_graph *u = &b->u;
+    cudaStream_t s = b->ctx->stream;
+    u->n = (uint32_t)n;
+    u->nnz = nnz;
+    {
+        DBuf<uint64_t> off64;
+        DBuf<uint32_t> dvoff;
+        DBuf<int> bad;
+        uint64_t *d64 = off64.ensure(n + 1);
+        int *dbad = bad.ensure(1);
+        MG_CUDA(cudaMemsetAsync(dbad, 0, sizeof(int), s));
+        MG_CUDA(cudaMemcpyAsync(d64, offsets, sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice, s));
+        MG_CUDA(cudaMemcpyAsync(dvoff.ensure(G + 1), b->voff.data(), sizeof(uint32_t) * (G + 1),
+                                cudaMemcpyHostToDevice, s));
+        uint32_t *dcol = u->col.ensure(nnz + 1);
+        if (nnz) MG_CUDA(cudaMemcpyAsync(dcol, cols, sizeof(uint32_t) * nnz, cudaMemcpyHostToDevice, s));
+        batch_rows_kernel<<<148 * 16, 256, 0, s>>>(d64, (uint32_t)n, dvoff.get(), G, dcol, u->off.ensure(n + 1),
+                                                   dbad);
+        MG_LAUNCH_CHECK();
+        int hbad = 0;
+        MG_CUDA(cudaMemcpyAsync(&hbad, dbad, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MG_CUDA(cudaStreamSynchronize(s));
+        MG_CHECK(!(hbad & 1), MG_ERR_INVALID, "offsets must be non-decreasing");
+        MG_CHECK(!(hbad & 2), MG_ERR_INVALID, "column index out of range");
+    }
+    if (weight_type == MG_WEIGHT_UNIT || unit) {
+        u->wk = WK_UNIT;
+    } else if (weight_type == MG_WEIGHT_F32) {
+        u->wk = WK_F32;
+        MG_CUDA(cudaMemcpyAsync(u->w32.ensure(nnz + 1), w, sizeof(float) * nnz, cudaMemcpyHostToDevice, s));
+    } else {
+        u->wk = WK_F64;
+        MG_CUDA(cudaMemcpyAsync(u->w64.ensure(nnz + 1), w, sizeof(double) * nnz, cudaMemcpyHostToDevice, s));
+    }
+    double total = 0;
+    int all_integral = 1;
+    for (uint32_t g = 0; g < G; g++) {
+        total += b->mass[g];
+        all_integral &= b->integral[g];
+    }
+    u->mass = total;
+    u->integral = all_integral;
+    MG_CUDA(cudaStreamSynchronize(s));
 }
 
 }  // namespace mg

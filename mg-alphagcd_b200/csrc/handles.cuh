@@ -55,6 +55,58 @@ struct mg_result {
 };
 
 namespace mg {
+// per-graph sums of one batched sweep
+struct GSum {
+    unsigned long long sin_u, s2_u;
+    double sin_f, s2_f;
+};
+// device-side control block of a batched run
+struct BatchCtrl {
+    int up;                     // direction of the next sweep
+    int active;                 // graphs taking part in the next sweep
+    unsigned long long sweeps;  // sweeps run
+    unsigned long long edges;   // entries of the graphs that took part in them
+    long long budget;           // sweeps left in this launch (CUDA-graph loop)
+    unsigned long long active_vertices;  // vertices of the graphs active in the next sweep
+    unsigned long long listed;  // vertices on the active lists (set by the host)
+    unsigned long long pad[2];  // pad[0]: blocks done in the decision kernel
+};
+// Device state of a batch, resident between runs.
+struct BatchWork {
+    DBuf<uint32_t> gid, goff, goff_new, goff0, gword, gnnz, loops, Cf;
+    // active lists: bins 0-8 entries (perm order) and vertices (id order), each
+    // with the graph of every entry; double-buffered for compaction
+    DBuf<uint32_t> lperm[2], lpgid[2], lvert[2], lvgid[2], flags, pos;
+    DBuf<double> sinv, curQ, gmass;
+    DBuf<GainK> gk;
+    DBuf<unsigned long long> iters;
+    DBuf<GSum> sums;
+    DBuf<BatchCtrl> ctrl;
+    BatchCtrl *h_ctrl = nullptr;  // pinned
+    ~BatchWork();
+};
+}  // namespace mg
+
+struct mg_batch {
+    mg_ctx *ctx = nullptr;
+    uint32_t graphs = 0;
+    mg_graph u;                     // the packed union: rows and columns in union ids
+    std::vector<uint32_t> voff;     // first vertex of each graph (graphs + 1)
+    std::vector<uint64_t> eoff;     // first entry of each graph (graphs + 1)
+    std::vector<double> mass;       // per graph
+    std::vector<int> integral;      // per graph
+    mg::BatchWork work;
+};
+
+struct mg_batch_result {
+    uint32_t graphs = 0;
+    mg_summary sum{};
+    std::vector<mg_batch_graph_summary> per;
+    std::vector<uint32_t> voff;        // first vertex of each graph
+    std::vector<uint32_t> assignment;  // graph-local community of every packed vertex
+};
+
+namespace mg {
 
 void ctx_prepare(mg_ctx *ctx);
 // graph construction
@@ -71,5 +123,10 @@ mg_status load_mtx_host(const char *path, uint32_t &n, std::vector<uint64_t> &of
                         std::vector<double> &w, std::string &err);
 // Louvain
 void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result &res);
+// batched form
+void batch_generate_sbm(mg_batch *b, const mg_sbm_params *params);
+void batch_from_host_csr(mg_batch *b, const uint64_t *voff, const uint64_t *offsets, const uint32_t *cols,
+                         const void *w, int weight_type);
+void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &res);
 
 }  // namespace mg

@@ -1,0 +1,1162 @@
+// lm_kernels.cuh -- the local-move sweep kernels and their launcher, shared by
+// the single-graph sweep (local_move.cu) and the batched sweep
+// (local_move_batch.cu).  Included by exactly those two translation units.
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "engine.cuh"
+
+namespace mg {
+namespace lmk {
+
+struct LMArgs {
+    const uint32_t *__restrict__ off;
+    const uint32_t *__restrict__ col;
+    const void *__restrict__ w;
+    const uint32_t *__restrict__ P;
+    uint32_t *__restrict__ N;
+    const double *__restrict__ k;
+    const double *__restrict__ sigma;
+    const uint32_t *__restrict__ perm;
+    GainK K;             // gain constants of the graph
+    int up;
+    int integral;
+    SweepAcc *acc;
+    // batched sweeps: graph of each vertex, per-graph control word and gain
+    // constants, the three assignment buffers, sum_in per vertex, and the
+    // sweep direction in device memory
+    const uint32_t *__restrict__ gid;
+    const uint32_t *__restrict__ pgid;  // graph of each entry of perm
+    const uint32_t *__restrict__ gword;
+    const GainK *__restrict__ gk;
+    uint32_t *Cb0, *Cb1, *Cb2;
+    double *__restrict__ sinv;
+    const int *__restrict__ up_dev;
+};
+
+// Per-vertex view of a sweep: the assignment read (P) and written (N) and the
+// gain constants.  A batched sweep takes them from the vertex's graph and
+// skips the vertices of graphs that are not active.
+struct VView {
+    const uint32_t *P;
+    uint32_t *N;
+    GainK K;
+};
+
+__device__ __forceinline__ uint32_t *buf_sel(const LMArgs &A, uint32_t b) {
+    return b == 0 ? A.Cb0 : b == 1 ? A.Cb1 : A.Cb2;
+}
+
+template <int BT>
+__device__ __forceinline__ bool vview_g(const LMArgs &A, uint32_t g, VView &v) {
+    if constexpr (BT == 0) {
+        v.P = A.P;
+        v.N = A.N;
+        return true;
+    } else {
+        const uint32_t w = A.gword[g];
+        if (!(w & kGwActive)) return false;
+        v.P = buf_sel(A, gw_p(w));
+        v.N = buf_sel(A, gw_n(w));
+        v.K = A.gk[g];
+        return true;
+    }
+}
+
+// vertex i, graph from the per-vertex table
+template <int BT>
+__device__ __forceinline__ bool vview(const LMArgs &A, uint32_t i, VView &v) {
+    return vview_g<BT>(A, BT ? A.gid[i] : 0u, v);
+}
+
+// entry pos of the bins list, graph from the list's own table
+template <int BT>
+__device__ __forceinline__ bool vview_at(const LMArgs &A, uint32_t pos, VView &v) {
+    return vview_g<BT>(A, BT ? A.pgid[pos] : 0u, v);
+}
+
+template <int BT>
+__device__ __forceinline__ const GainK &kref(const LMArgs &A, const VView &v) {
+    if constexpr (BT == 0) return A.K;
+    else return v.K;
+}
+
+template <int BT>
+__device__ __forceinline__ int load_up(const LMArgs &A) {
+    if constexpr (BT == 0) return A.up;
+    else return *A.up_dev;
+}
+
+// sum_in contribution of vertex i: into the thread's running sum (single
+// graph) or into the per-vertex array (batched; summed per graph later)
+template <int BT>
+__device__ __forceinline__ void put_sin(const LMArgs &A, uint32_t i, double &sin, double x) {
+    if constexpr (BT == 0) sin += x;
+    else A.sinv[i] = x;
+}
+
+template <int WK>
+__device__ __forceinline__ double wload(const void *w, uint32_t e) {
+    if constexpr (WK == WK_UNIT) return 1.0;
+    else if constexpr (WK == WK_F32 || WK == WK_F32I) return (double)__ldcs((const float *)w + e);
+    else return __ldcs((const double *)w + e);
+}
+
+// ---- gain in the three precision modes -------------------------------------
+template <int PREC>
+struct Prec;
+template <>
+struct Prec<MG_PREC_FP64> {
+    using G = double;
+    // (k_ic - (e - k_i*(a - s_c)/(2m))) / m, each operation rounded as written;
+    // both quotients are correctly rounded (div_by), so the value is the one a
+    // divide instruction gives
+    __device__ static __forceinline__ G gain(double kic, double e, double ki, double a, double sc,
+                                             const GainK &K) {
+        double t = __dmul_rn(ki, __dsub_rn(a, sc));
+        t = div_by(t, K.two_m, K.r_two_m);
+        t = __dsub_rn(e, t);
+        return div_by(__dsub_rn(kic, t), K.m, K.r_m);
+    }
+};
+template <>
+struct Prec<MG_PREC_FP32> {
+    using G = float;
+    __device__ static __forceinline__ G gain(double kic, double e, double ki, double a, double sc,
+                                             const GainK &K) {
+        float t = __fmul_rn((float)ki, __fsub_rn((float)a, (float)sc));
+        t = div_by(t, K.two_m_f, K.r_two_m_f);
+        t = __fsub_rn((float)e, t);
+        return div_by(__fsub_rn((float)kic, t), K.m_f, K.r_m_f);
+    }
+};
+template <>
+struct Prec<MG_PREC_INT64> {
+    using G = long long;
+    // 2m*m*gain = 2m*(k_ic - e) + k_i*(a - s_c), exact for integral weights
+    __device__ static __forceinline__ G gain(double kic, double e, double ki, double a, double sc,
+                                             const GainK &K) {
+        return K.mass_i * ((long long)kic - (long long)e) + (long long)ki * ((long long)a - (long long)sc);
+    }
+};
+
+template <class G>
+__device__ __forceinline__ bool better(G g2, uint32_t c2, G g1, uint32_t c1, int up) {
+    return g2 > g1 || (g2 == g1 && (up ? c2 < c1 : c2 > c1));
+}
+
+template <int VER>
+__device__ __forceinline__ bool is_candidate(uint32_t c, uint32_t src, int up) {
+    if constexpr (VER == 1) return up ? c < src : c > src;
+    else return c != src;
+}
+
+template <int VER>
+__device__ __forceinline__ uint32_t final_choice(uint32_t dst, uint32_t src, int up) {
+    if constexpr (VER == 1) return dst;
+    else return up ? (dst < src ? dst : src) : (dst > src ? dst : src);
+}
+
+template <class G>
+__device__ __forceinline__ G shfl_xor_g(G v, int o) {
+    return __shfl_xor_sync(0xffffffffu, v, o);
+}
+
+// Block-level accumulation of sum_in / distinct into the sweep accumulators.
+__device__ __forceinline__ void flush_acc(SweepAcc *acc, int integral, double sin, unsigned dcnt) {
+    __shared__ double s_f;
+    __shared__ unsigned long long s_d;
+    if (threadIdx.x == 0) {
+        s_f = 0;
+        s_d = 0;
+    }
+    __syncthreads();
+    double v = warp_sum(sin);
+    unsigned long long d = warp_sum((unsigned long long)dcnt);
+    if ((threadIdx.x & 31) == 0) {
+        if (v != 0) atomicAdd(&s_f, v);
+        if (d) atomicAdd(&s_d, d);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (integral) {
+            if (s_f != 0) atomicAdd(&acc->sin_u, (unsigned long long)s_f);
+        } else if (s_f != 0) {
+            atomicAdd(&acc->sin_f, s_f);
+        }
+        if (s_d) atomicAdd(&acc->distinct, s_d);
+    }
+}
+
+// ============================================================================
+// bins 0-4: T lanes per vertex, deg <= T
+// ============================================================================
+template <int T, int WK, int PREC, int VER, int BT>
+__global__ void __launch_bounds__(256) lm_tile_kernel(LMArgs A, uint32_t bin_off, uint32_t bin_size) {
+    using G = typename Prec<PREC>::G;
+    const int up = load_up<BT>(A);
+    __shared__ double wbuf[8][32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t gl = lane & (T - 1), gbase = lane & ~(uint32_t)(T - 1);
+    const uint32_t gmask = T == 32 ? 0xffffffffu : (((1u << T) - 1u) << gbase);
+    constexpr uint32_t GPW = 32 / T;
+    double sin = 0;
+    unsigned dcnt = 0;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarp = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t wb = gwarp * GPW; wb < bin_size; wb += nwarp * GPW) {
+        const uint32_t idx = wb + lane / T;
+        bool active = idx < bin_size;
+        uint32_t i = 0, src = 0, lo = 0, hi = 0;
+        double ki = 0, a = 0;
+        VView vv;
+        if (active) {
+            i = A.perm[bin_off + idx];
+            active = vview_at<BT>(A, bin_off + idx, vv);
+        }
+        if (active) {
+            lo = A.off[i];
+            hi = A.off[i + 1];
+            src = vv.P[i];
+        }
+        const uint32_t e = lo + gl;
+        const bool has = active && e < hi;
+        uint32_t j = kEmpty, c = kEmpty;
+        double w = 0;
+        if (has) {
+            j = __ldcs(A.col + e);
+            w = wload<WK>(A.w, e);
+            c = vv.P[j];
+        }
+        if (active) {
+            ki = A.k[i];
+            a = A.sigma[src] - ki;
+        }
+        const bool self = has && j == i;
+        const bool inner = has && !self && c == src;
+        const bool cand = has && c != src && is_candidate<VER>(c, src, up);
+        const uint32_t key = cand ? c : kEmpty;
+        const uint32_t peers = __match_any_sync(0xffffffffu, key) & gmask;
+        const bool leader = cand && (uint32_t)(__ffs(peers) - 1) == lane;
+        double kic, e_src, selfw;
+        if constexpr (WK == WK_UNIT) {
+            kic = u2d(__popc(peers));
+            e_src = u2d(__popc(__ballot_sync(0xffffffffu, inner) & gmask));
+            selfw = u2d(__popc(__ballot_sync(0xffffffffu, self) & gmask));
+        } else {
+            wbuf[warp][lane] = w;
+            __syncwarp();
+            kic = 0;
+            if (leader) {
+                uint32_t mset = peers;
+                while (mset) {
+                    int l = __ffs(mset) - 1;
+                    kic += wbuf[warp][l];
+                    mset &= mset - 1;
+                }
+            }
+            __syncwarp();
+            e_src = inner ? w : 0.0;
+            selfw = self ? w : 0.0;
+#pragma unroll
+            for (int o = T / 2; o > 0; o >>= 1) {
+                e_src += __shfl_xor_sync(0xffffffffu, e_src, o);
+                selfw += __shfl_xor_sync(0xffffffffu, selfw, o);
+            }
+        }
+        G best = G(0);
+        uint32_t dst = src;
+        if (leader) {
+            G g = Prec<PREC>::gain(kic, e_src, ki, a, A.sigma[c], kref<BT>(A, vv));
+            if (better(g, c, best, dst, up)) {
+                best = g;
+                dst = c;
+            }
+            dcnt++;
+        }
+#pragma unroll
+        for (int o = T / 2; o > 0; o >>= 1) {
+            G g2 = shfl_xor_g(best, o);
+            uint32_t c2 = __shfl_xor_sync(0xffffffffu, dst, o);
+            if (better(g2, c2, best, dst, up)) {
+                best = g2;
+                dst = c2;
+            }
+        }
+        if (active && gl == 0) {
+            vv.N[i] = final_choice<VER>(dst, src, up);
+            put_sin<BT>(A, i, sin, e_src + selfw);
+        }
+    }
+    flush_acc(A.acc, A.integral, sin, dcnt);
+}
+
+// ============================================================================
+// bins 5-8: GT threads per vertex, SLOTS-entry shared table
+// ============================================================================
+// table value type: 32-bit integer sums for integral weights, else double
+template <int WK>
+struct ValT {
+    using type = typename std::conditional<kIntg<WK>, uint32_t, double>::type;
+};
+
+template <int GT>
+__device__ __forceinline__ void group_sync() {
+    if constexpr (GT == 32) __syncwarp();
+    else __syncthreads();
+}
+
+// Two sums over a group of GT threads with one pair of barriers; results
+// valid in every thread.  red: 2 * 32 doubles.
+template <int GT>
+__device__ __forceinline__ void group_sum2(double &a, double &b, double *red) {
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if constexpr (GT > 32) {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (lane == 0) {
+            red[warp] = a;
+            red[32 + warp] = b;
+        }
+        __syncthreads();
+        double ta = 0, tb = 0;
+#pragma unroll
+        for (int w2 = 0; w2 < GT / 32; w2++) {
+            ta += red[w2];
+            tb += red[32 + w2];
+        }
+        __syncthreads();
+        a = ta;
+        b = tb;
+    }
+}
+
+// Sum over a group of GT threads; result valid in every thread.
+template <int GT>
+__device__ __forceinline__ double group_sum(double v, double *red) {
+    v = warp_sum(v);
+    if constexpr (GT == 32) {
+        return v;
+    } else {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (lane == 0) red[warp] = v;
+        __syncthreads();
+        double t = 0;
+#pragma unroll
+        for (int w2 = 0; w2 < GT / 32; w2++) t += red[w2];
+        __syncthreads();
+        return t;
+    }
+}
+
+template <int GT, class G>
+__device__ __forceinline__ void group_argmax(G &best, uint32_t &dst, int up, G *rg, uint32_t *rc) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        G g2 = shfl_xor_g(best, o);
+        uint32_t c2 = __shfl_xor_sync(0xffffffffu, dst, o);
+        if (better(g2, c2, best, dst, up)) {
+            best = g2;
+            dst = c2;
+        }
+    }
+    if constexpr (GT > 32) {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (lane == 0) {
+            rg[warp] = best;
+            rc[warp] = dst;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int w2 = 0; w2 < GT / 32; w2++) {
+            if (better(rg[w2], rc[w2], best, dst, up)) {
+                best = rg[w2];
+                dst = rc[w2];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <int X>
+struct Log2 {
+    static constexpr int value = 1 + Log2<X / 2>::value;
+};
+template <>
+struct Log2<1> {
+    static constexpr int value = 0;
+};
+
+template <int SLOTS>
+__device__ __forceinline__ uint32_t table_find_or_insert(uint32_t *keys, uint32_t c, int bits) {
+    const uint32_t mask = (1u << bits) - 1u;
+    uint32_t h = hash_slot(c, bits);
+    for (int p = 0; p < SLOTS; p++) {
+        uint32_t cur = ((volatile uint32_t *)keys)[h];
+        if (cur == c) return h;
+        if (cur == kEmpty) {
+            uint32_t prev = atomicCAS(keys + h, kEmpty, c);
+            if (prev == kEmpty || prev == c) return h;
+        }
+        h = (h + 1) & mask;
+    }
+    return kEmpty;  // unreachable: tables hold >= 2*deg slots
+}
+
+// table bits for a vertex of degree d: 2*d slots rounded up to a power of
+// two, at least 32, at most the group's table
+template <int SLOTS>
+__device__ __forceinline__ int table_bits(uint32_t d) {
+    const int want = d <= 16 ? 5 : 33 - __clz(2 * d - 1);
+    return want < Log2<SLOTS>::value ? want : Log2<SLOTS>::value;
+}
+
+// weight of edge e as the table's value type: exact 32-bit integer for
+// integral graphs (no float->int conversion instruction: the f64 value plus
+// 2^52 carries the integer in its low mantissa word), double otherwise
+template <int WK>
+__device__ __forceinline__ typename ValT<WK>::type wget(const void *w, uint32_t e) {
+    if constexpr (WK == WK_UNIT) return 1u;
+    else if constexpr (WK == WK_F64I)
+        return (uint32_t)__double2loint(__dadd_rn(__ldcs((const double *)w + e), 4503599627370496.0));
+    else if constexpr (WK == WK_F32I) return __float2uint_rn(__ldcs((const float *)w + e));
+    else return wload<WK>(w, e);
+}
+
+template <class V>
+__device__ __forceinline__ double v2d(V v) {
+    if constexpr (std::is_same<V, uint32_t>::value) return u2d(v);
+    else return v;
+}
+
+// Shared-memory hash table per group of GT threads.  Newly inserted slots are
+// appended to a per-table list, so the evaluation runs densely over the
+// distinct candidates only (and resets exactly those slots).
+template <int GT, int SLOTS, int WK, int PREC, int VER, int BLOCK, int BT>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) lm_hash_kernel(LMArgs A, uint32_t bin_off, uint32_t bin_size) {
+    using G = typename Prec<PREC>::G;
+    const int up = load_up<BT>(A);
+    using V = typename ValT<WK>::type;
+    constexpr int GPB = BLOCK / GT;
+    constexpr int BATCH = 4;
+    constexpr int EB = 4;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t *keys_all = (uint32_t *)smem_raw;
+    V *vals_all = (V *)(smem_raw + sizeof(uint32_t) * SLOTS * GPB);
+    uint16_t *used_all = (uint16_t *)(smem_raw + (sizeof(uint32_t) + sizeof(V)) * SLOTS * GPB);
+    __shared__ V acc_e[GPB], acc_s[GPB];
+    __shared__ uint32_t cnt[GPB];
+    __shared__ G red_g[32];
+    __shared__ uint32_t red_c[32];
+    const int g = threadIdx.x / GT, t = threadIdx.x % GT;
+    uint32_t *keys = keys_all + g * SLOTS;
+    V *vals = vals_all + g * SLOTS;
+    uint16_t *used = used_all + g * (SLOTS / 2);
+    for (int s2 = threadIdx.x; s2 < SLOTS * GPB; s2 += BLOCK) {
+        keys_all[s2] = kEmpty;
+        vals_all[s2] = V(0);
+    }
+    if (threadIdx.x < GPB) {
+        acc_e[threadIdx.x] = V(0);
+        acc_s[threadIdx.x] = V(0);
+        cnt[threadIdx.x] = 0;
+    }
+    __syncthreads();
+    double sin = 0;
+    unsigned dcnt = 0;
+    for (uint32_t idx = blockIdx.x * GPB + g; idx - g < bin_size; idx += gridDim.x * GPB) {
+        // the loop condition is uniform inside a group (GT == 32) or block (GT > 32)
+        bool active = idx < bin_size;
+        uint32_t i = 0, src = 0, lo = 0, hi = 0;
+        double ki = 0, a = 0;
+        VView vv;
+        if (active) {
+            i = A.perm[bin_off + idx];
+            active = vview_at<BT>(A, bin_off + idx, vv);
+        }
+        if (active) {
+            lo = A.off[i];
+            hi = A.off[i + 1];
+            src = vv.P[i];
+            ki = A.k[i];
+            a = A.sigma[src] - ki;  // issued early, consumed after the edge pass
+        }
+        const int tb = table_bits<SLOTS>(hi - lo);
+        V e_part = V(0), s_part = V(0);
+        for (uint32_t base = lo + t; base < hi; base += GT * BATCH) {
+            uint32_t jj[BATCH], cc[BATCH];
+            V ww[BATCH];
+#pragma unroll
+            for (int b = 0; b < BATCH; b++) {
+                uint32_t e = base + b * GT;
+                jj[b] = e < hi ? __ldcs(A.col + e) : kEmpty;
+                ww[b] = e < hi ? wget<WK>(A.w, e) : V(0);
+            }
+#pragma unroll
+            for (int b = 0; b < BATCH; b++) cc[b] = jj[b] != kEmpty ? vv.P[jj[b]] : kEmpty;
+#pragma unroll
+            for (int b = 0; b < BATCH; b++) {
+                if (jj[b] == kEmpty) continue;
+                const uint32_t c = cc[b];
+                if (c != src) {
+                    if (is_candidate<VER>(c, src, up)) {
+                        const uint32_t mask = (1u << tb) - 1u;
+                        uint32_t h = hash_slot(c, tb);
+                        for (int p = 0; p < SLOTS; p++) {
+                            uint32_t cur = ((volatile uint32_t *)keys)[h];
+                            if (cur == c) break;
+                            if (cur == kEmpty) {
+                                uint32_t prev = atomicCAS(keys + h, kEmpty, c);
+                                if (prev == kEmpty) {
+                                    used[atomicAdd(cnt + g, 1u)] = (uint16_t)h;
+                                    break;
+                                }
+                                if (prev == c) break;
+                            }
+                            h = (h + 1) & mask;
+                        }
+                        atomicAdd(vals + h, ww[b]);
+                    }
+                } else if (jj[b] != i) {
+                    e_part += ww[b];
+                } else {
+                    s_part += ww[b];
+                }
+            }
+        }
+        // group totals of e and self weight, folded into the barrier that
+        // publishes the table
+        e_part = warp_sum(e_part);
+        s_part = warp_sum(s_part);
+        if ((threadIdx.x & 31) == 0) {
+            if (e_part != V(0)) atomicAdd(acc_e + g, e_part);
+            if (s_part != V(0)) atomicAdd(acc_s + g, s_part);
+        }
+        group_sync<GT>();
+        const double e_src = v2d(acc_e[g]), selfw = v2d(acc_s[g]);
+        const uint32_t nd = cnt[g];
+        G best = G(0);
+        uint32_t dst = src;
+        for (uint32_t u0 = t; u0 < nd; u0 += GT * EB) {
+            uint32_t kk[EB];
+            double sc[EB], kv[EB];
+#pragma unroll
+            for (int b = 0; b < EB; b++) {
+                const uint32_t u = u0 + b * GT;
+                kk[b] = kEmpty;
+                if (u < nd) {
+                    const uint32_t h = used[u];
+                    kk[b] = keys[h];
+                    kv[b] = v2d(vals[h]);
+                    keys[h] = kEmpty;
+                    vals[h] = V(0);
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < EB; b++)
+                if (kk[b] != kEmpty) sc[b] = A.sigma[kk[b]];
+#pragma unroll
+            for (int b = 0; b < EB; b++) {
+                if (kk[b] != kEmpty) {
+                    G gn = Prec<PREC>::gain(kv[b], e_src, ki, a, sc[b], kref<BT>(A, vv));
+                    if (better(gn, kk[b], best, dst, up)) {
+                        best = gn;
+                        dst = kk[b];
+                    }
+                }
+            }
+        }
+        group_argmax<GT, G>(best, dst, up, red_g, red_c);
+        if (t == 0) {
+            if (active) {
+                vv.N[i] = final_choice<VER>(dst, src, up);
+                put_sin<BT>(A, i, sin, e_src + selfw);
+                dcnt += nd;
+            }
+            cnt[g] = 0;
+            acc_e[g] = V(0);
+            acc_s[g] = V(0);
+        }
+        group_sync<GT>();
+    }
+    flush_acc(A.acc, A.integral, sin, dcnt);
+}
+
+// ============================================================================
+// bin 9, tiers 0-4: one vertex per thread-block cluster of CS CTAs, the
+// cluster's distributed shared memory holding one hash table of CS *
+// kClusterSlots slots.  A neighbour community hashes to (owner CTA, slot);
+// inserts into other CTAs' segments go through DSMEM atomics; each CTA then
+// evaluates the candidates of its own segment, and rank 0 reduces the CS
+// winners.  Two cluster barriers per vertex (accumulators double-buffered).
+// Unit weights use packed 64-bit slots {key:32 | count:32}.
+// ============================================================================
+namespace cg = cooperative_groups;
+constexpr int kClusterThreads = 1024;  // one CTA per SM with a 16K-slot segment
+constexpr uint64_t kEmpty64 = 0xFFFFFFFF00000000ull;
+
+template <int CS>
+__device__ __forceinline__ void cluster_barrier() {
+    if constexpr (CS == 1) __syncthreads();
+    else cg::this_cluster().sync();
+}
+
+template <int CS, class T>
+__device__ __forceinline__ T *rank_ptr(T *p, unsigned r) {
+    if constexpr (CS == 1) return p;
+    else return cg::this_cluster().map_shared_rank(p, r);
+}
+
+template <int CS, int WK, int PREC, int VER, int BT>
+__global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A, const uint32_t *verts,
+                                                                        uint32_t count) {
+    using G = typename Prec<PREC>::G;
+    const int up = load_up<BT>(A);
+    constexpr int S = kClusterSlots;
+    constexpr int BATCH = 4;
+    constexpr int EB = 4;  // slots per thread per evaluation batch
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint64_t *packed = (uint64_t *)smem_raw;                 // integral weights
+    uint32_t *keys = (uint32_t *)smem_raw;                   // real weights
+    double *vals = (double *)(smem_raw + sizeof(uint32_t) * S);
+    // slots of this CTA's segment that received a new key, in insertion order
+    uint16_t *used = (uint16_t *)(smem_raw + (kIntg<WK> ? sizeof(uint64_t) : sizeof(uint32_t) + sizeof(double)) * S);
+    __shared__ uint32_t ucnt;
+    __shared__ double acc_e[2], acc_s[2];
+    __shared__ G best_g[2][CS];
+    __shared__ uint32_t best_c[2][CS];
+    __shared__ G red_g[32];
+    __shared__ uint32_t red_c[32];
+    unsigned rank = 0;
+    if constexpr (CS > 1) rank = cg::this_cluster().block_rank();
+    for (int s = threadIdx.x; s < S; s += kClusterThreads) {
+        if constexpr (kIntg<WK>) packed[s] = kEmpty64;
+        else {
+            keys[s] = kEmpty;
+            vals[s] = 0.0;
+        }
+    }
+    if (threadIdx.x < 2) {
+        acc_e[threadIdx.x] = 0;
+        acc_s[threadIdx.x] = 0;
+    }
+    if (threadIdx.x == 0) ucnt = 0;
+    cluster_barrier<CS>();
+    const uint32_t cluster_id = blockIdx.x / CS, nclusters = gridDim.x / CS;
+    const uint32_t tc = rank * kClusterThreads + threadIdx.x;
+    constexpr uint32_t stride = CS * kClusterThreads;
+    double sin = 0;
+    unsigned dcnt = 0;
+    int par = 0;
+    for (uint32_t vi = cluster_id; vi < count; vi += nclusters) {
+        const uint32_t i = verts[vi];
+        VView vv;
+        // uniform over the cluster: every CTA works on the same vertex
+        if (!vview<BT>(A, i, vv)) continue;
+        const uint32_t lo = A.off[i], hi = A.off[i + 1], src = vv.P[i];
+        const double ki = A.k[i];
+        const double a = A.sigma[src] - ki;
+        double e_part = 0, s_part = 0;
+        for (uint32_t base = lo + tc; base < hi; base += stride * BATCH) {
+            uint32_t jj[BATCH], cc[BATCH];
+            double ww[BATCH];
+#pragma unroll
+            for (int b = 0; b < BATCH; b++) {
+                uint32_t e = base + b * stride;
+                jj[b] = e < hi ? __ldcs(A.col + e) : kEmpty;
+                ww[b] = e < hi ? wload<WK>(A.w, e) : 0.0;
+            }
+#pragma unroll
+            for (int b = 0; b < BATCH; b++) cc[b] = jj[b] != kEmpty ? vv.P[jj[b]] : kEmpty;
+#pragma unroll
+            for (int b = 0; b < BATCH; b++) {
+                if (jj[b] == kEmpty) continue;
+                const uint32_t c = cc[b];
+                if (c != src) {
+                    if (!is_candidate<VER>(c, src, up)) continue;
+                    const uint32_t h = hash_range(c, (uint32_t)CS * S);
+                    const unsigned owner = h / S;
+                    uint32_t s = h & (S - 1);
+                    if constexpr (kIntg<WK>) {
+                        const unsigned long long wi = (uint32_t)ww[b];
+                        uint64_t *seg = rank_ptr<CS>(packed, owner);
+                        bool placed = false;
+                        for (int p = 0; p < S; p++) {
+                            uint64_t cur = ((volatile uint64_t *)seg)[s];
+                            uint32_t k = (uint32_t)(cur >> 32);
+                            if (k == c) {
+                                atomicAdd((unsigned long long *)(seg + s), wi);
+                                placed = true;
+                                break;
+                            }
+                            if (k == kEmpty) {
+                                uint64_t prev = atomicCAS((unsigned long long *)(seg + s), kEmpty64,
+                                                          ((uint64_t)c << 32) | wi);
+                                if (prev == kEmpty64) {
+                                    rank_ptr<CS>(used, owner)[atomicAdd(rank_ptr<CS>(&ucnt, owner), 1u)] =
+                                        (uint16_t)s;
+                                    placed = true;
+                                    break;
+                                }
+                                if ((uint32_t)(prev >> 32) == c) {
+                                    atomicAdd((unsigned long long *)(seg + s), wi);
+                                    placed = true;
+                                    break;
+                                }
+                            }
+                            s = (s + 1) & (S - 1);
+                        }
+                        if (!placed) atomicAdd(&A.acc->overflow, 1ull);
+                    } else {
+                        uint32_t *ks = rank_ptr<CS>(keys, owner);
+                        double *vs = rank_ptr<CS>(vals, owner);
+                        bool placed = false;
+                        for (int p = 0; p < S; p++) {
+                            uint32_t cur = ((volatile uint32_t *)ks)[s];
+                            if (cur == c) {
+                                placed = true;
+                                break;
+                            }
+                            if (cur == kEmpty) {
+                                uint32_t prev = atomicCAS(ks + s, kEmpty, c);
+                                if (prev == kEmpty) {
+                                    rank_ptr<CS>(used, owner)[atomicAdd(rank_ptr<CS>(&ucnt, owner), 1u)] =
+                                        (uint16_t)s;
+                                    placed = true;
+                                    break;
+                                }
+                                if (prev == c) {
+                                    placed = true;
+                                    break;
+                                }
+                            }
+                            s = (s + 1) & (S - 1);
+                        }
+                        if (placed) atomicAdd(vs + s, ww[b]);
+                        else atomicAdd(&A.acc->overflow, 1ull);
+                    }
+                } else if (jj[b] != i) {
+                    e_part += ww[b];
+                } else {
+                    s_part += ww[b];
+                }
+            }
+        }
+        e_part = warp_sum(e_part);
+        s_part = warp_sum(s_part);
+        if ((threadIdx.x & 31) == 0) {
+            if (e_part != 0) atomicAdd(rank_ptr<CS>(&acc_e[par], 0), e_part);
+            if (s_part != 0) atomicAdd(rank_ptr<CS>(&acc_s[par], 0), s_part);
+        }
+        cluster_barrier<CS>();  // all inserts and partial sums are in
+        const double e_src = *rank_ptr<CS>(&acc_e[par], 0);
+        G best = G(0);
+        uint32_t dst = src;
+        const uint32_t nd = ucnt;
+        for (uint32_t u0 = threadIdx.x; u0 < nd; u0 += kClusterThreads * EB) {
+            uint32_t kk[EB];
+            double kv[EB], sc[EB];
+#pragma unroll
+            for (int b = 0; b < EB; b++) {
+                const uint32_t u = u0 + b * kClusterThreads;
+                kk[b] = kEmpty;
+                if (u < nd) {
+                    const uint32_t s = used[u];
+                    if constexpr (kIntg<WK>) {
+                        uint64_t v = packed[s];
+                        kk[b] = (uint32_t)(v >> 32);
+                        kv[b] = u2d((uint32_t)v);
+                        packed[s] = kEmpty64;
+                    } else {
+                        kk[b] = keys[s];
+                        kv[b] = vals[s];
+                        keys[s] = kEmpty;
+                        vals[s] = 0.0;
+                    }
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < EB; b++)
+                if (kk[b] != kEmpty) sc[b] = A.sigma[kk[b]];
+#pragma unroll
+            for (int b = 0; b < EB; b++) {
+                if (kk[b] != kEmpty) {
+                    G gn = Prec<PREC>::gain(kv[b], e_src, ki, a, sc[b], kref<BT>(A, vv));
+                    if (better(gn, kk[b], best, dst, up)) {
+                        best = gn;
+                        dst = kk[b];
+                    }
+                }
+            }
+        }
+        group_argmax<kClusterThreads, G>(best, dst, up, red_g, red_c);
+        if (threadIdx.x == 0) {
+            dcnt += nd;
+            ucnt = 0;  // every thread of this CTA has read it (barriers in group_argmax)
+            rank_ptr<CS>(&best_g[par][0], 0)[rank] = best;
+            rank_ptr<CS>(&best_c[par][0], 0)[rank] = dst;
+        }
+        cluster_barrier<CS>();  // winners of every CTA are with rank 0
+        if (rank == 0 && threadIdx.x == 0) {
+            G bg = G(0);
+            uint32_t bc = src;
+            for (int r = 0; r < CS; r++)
+                if (better(best_g[par][r], best_c[par][r], bg, bc, up)) {
+                    bg = best_g[par][r];
+                    bc = best_c[par][r];
+                }
+            vv.N[i] = final_choice<VER>(bc, src, up);
+            put_sin<BT>(A, i, sin, e_src + acc_s[par]);
+            acc_e[par] = 0;
+            acc_s[par] = 0;
+        }
+        par ^= 1;
+    }
+    cluster_barrier<CS>();  // no CTA leaves while others may still touch its memory
+    flush_acc(A.acc, A.integral, sin, dcnt);
+}
+
+// ============================================================================
+// bin 9, last tier (giants): global tables, many CTAs per vertex
+// ============================================================================
+constexpr int kHeavyThreads = 256;
+constexpr uint32_t kHeavyChunkE = 4096;  // edges per insert item
+constexpr uint32_t kHeavyChunkS = 4096;  // slots per evaluate item
+
+__device__ __forceinline__ uint32_t find_item(const uint32_t *item_off, uint32_t H, uint32_t q) {
+    // last h with item_off[h] <= q
+    uint32_t lo = 0, hi = H;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (item_off[mid] <= q) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+
+template <int WK, int VER, int BT>
+__global__ void __launch_bounds__(kHeavyThreads) heavy_insert_kernel(LMArgs A, const uint32_t *hv, uint32_t H,
+                                                                      const uint32_t *ins_off,
+                                                                      const uint64_t *toff,
+                                                                      const uint32_t *tsize, uint32_t *tkeys,
+                                                                      double *tvals, double *hacc) {
+    constexpr int BATCH = 4;
+    __shared__ double red[2][kHeavyThreads / 32];
+    const uint32_t q = blockIdx.x;
+    const uint32_t h = find_item(ins_off, H, q);
+    const uint32_t v = hv[h];
+    VView vv;
+    if (!vview<BT>(A, v, vv)) return;  // uniform over the block
+    const int up = load_up<BT>(A);
+    const uint32_t chunk = q - ins_off[h];
+    const uint32_t vlo = A.off[v], vhi = A.off[v + 1];
+    const uint32_t lo = vlo + chunk * kHeavyChunkE;
+    const uint32_t hi = min(vhi, lo + kHeavyChunkE);
+    const uint32_t src = vv.P[v];
+    const uint32_t ts = tsize[h];
+    uint32_t *keys = tkeys + toff[h];
+    double *vals = tvals + toff[h];
+    double e_part = 0, s_part = 0;
+    for (uint32_t base = lo + threadIdx.x; base < hi; base += kHeavyThreads * BATCH) {
+        uint32_t jj[BATCH], cc[BATCH];
+        double ww[BATCH];
+#pragma unroll
+        for (int b = 0; b < BATCH; b++) {
+            uint32_t e = base + b * kHeavyThreads;
+            jj[b] = e < hi ? __ldcs(A.col + e) : kEmpty;
+            ww[b] = e < hi ? wload<WK>(A.w, e) : 0.0;
+        }
+#pragma unroll
+        for (int b = 0; b < BATCH; b++) cc[b] = jj[b] != kEmpty ? vv.P[jj[b]] : kEmpty;
+#pragma unroll
+        for (int b = 0; b < BATCH; b++) {
+            if (jj[b] == kEmpty) continue;
+            const uint32_t c = cc[b];
+            if (c != src) {
+                if (is_candidate<VER>(c, src, up)) {
+                    uint32_t s = hash_range(c, ts);
+                    for (uint32_t p = 0; p < ts; p++) {
+                        uint32_t cur = ((volatile uint32_t *)keys)[s];
+                        if (cur == c) break;
+                        if (cur == kEmpty) {
+                            uint32_t prev = atomicCAS(keys + s, kEmpty, c);
+                            if (prev == kEmpty || prev == c) break;
+                        }
+                        s = s + 1 == ts ? 0 : s + 1;
+                    }
+                    atomicAdd(vals + s, ww[b]);
+                }
+            } else if (jj[b] != v) {
+                e_part += ww[b];
+            } else {
+                s_part += ww[b];
+            }
+        }
+    }
+    e_part = warp_sum(e_part);
+    s_part = warp_sum(s_part);
+    if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = e_part;
+        red[1][threadIdx.x >> 5] = s_part;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, b = 0;
+        for (int w2 = 0; w2 < kHeavyThreads / 32; w2++) {
+            a += red[0][w2];
+            b += red[1][w2];
+        }
+        if (a != 0) atomicAdd(hacc + 2 * h, a);
+        if (b != 0) atomicAdd(hacc + 2 * h + 1, b);
+    }
+}
+
+// per evaluate item: packed winner {gain bits, id}
+template <int PREC, int BT>
+__global__ void __launch_bounds__(kHeavyThreads) heavy_eval_kernel(LMArgs A, const uint32_t *hv, uint32_t H,
+                                                                    const uint32_t *eval_off,
+                                                                    const uint64_t *toff, const uint32_t *tsize,
+                                                                    uint32_t *tkeys, double *tvals,
+                                                                    const double *hacc,
+                                                                    unsigned long long *item_best) {
+    using G = typename Prec<PREC>::G;
+    __shared__ G rg[32];
+    __shared__ uint32_t rc[32];
+    __shared__ unsigned long long s_d;
+    const uint32_t q = blockIdx.x;
+    const uint32_t h = find_item(eval_off, H, q);
+    const uint32_t v = hv[h];
+    VView vv;
+    if (!vview<BT>(A, v, vv)) return;  // uniform over the block
+    const int up = load_up<BT>(A);
+    const uint32_t part = q - eval_off[h];
+    const uint32_t ts = tsize[h];
+    const uint32_t lo = part * kHeavyChunkS, hi = min(ts, lo + kHeavyChunkS);
+    uint32_t *keys = tkeys + toff[h];
+    double *vals = tvals + toff[h];
+    const uint32_t src = vv.P[v];
+    const double ki = A.k[v];
+    const double a = A.sigma[src] - ki;
+    const double e_src = hacc[2 * h];
+    if (threadIdx.x == 0) s_d = 0;
+    G best = G(0);
+    uint32_t dst = src;
+    unsigned dcnt = 0;
+    for (uint32_t s = lo + threadIdx.x; s < hi; s += kHeavyThreads) {
+        uint32_t c = keys[s];
+        if (c != kEmpty) {
+            double kv = vals[s];
+            keys[s] = kEmpty;
+            vals[s] = 0.0;
+            G gn = Prec<PREC>::gain(kv, e_src, ki, a, A.sigma[c], kref<BT>(A, vv));
+            if (better(gn, c, best, dst, up)) {
+                best = gn;
+                dst = c;
+            }
+            dcnt++;
+        }
+    }
+    group_argmax<kHeavyThreads, G>(best, dst, up, rg, rc);
+    unsigned long long d = warp_sum((unsigned long long)dcnt);
+    if ((threadIdx.x & 31) == 0 && d) atomicAdd(&s_d, d);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long bits;
+        if constexpr (sizeof(G) == 8) bits = *(unsigned long long *)&best;
+        else bits = (unsigned long long)(*(uint32_t *)&best);
+        item_best[2 * q] = bits;
+        item_best[2 * q + 1] = dst;
+        if (s_d) atomicAdd(&A.acc->distinct, s_d);
+    }
+}
+
+template <int PREC, int VER, int BT>
+__global__ void heavy_final_kernel(LMArgs A, const uint32_t *hv, uint32_t H, const uint32_t *eval_off,
+                                   double *hacc, const unsigned long long *item_best) {
+    using G = typename Prec<PREC>::G;
+    const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    const int up = load_up<BT>(A);
+    double sin = 0;
+    VView vv;
+    if (h < H && vview<BT>(A, hv[h], vv)) {
+        const uint32_t v = hv[h];
+        const uint32_t src = vv.P[v];
+        G best = G(0);
+        uint32_t dst = src;
+        for (uint32_t q = eval_off[h]; q < eval_off[h + 1]; q++) {
+            unsigned long long bits = item_best[2 * q];
+            uint32_t c = (uint32_t)item_best[2 * q + 1];
+            G g;
+            if constexpr (sizeof(G) == 8) g = *(G *)&bits;
+            else {
+                uint32_t b32 = (uint32_t)bits;
+                g = *(G *)&b32;
+            }
+            if (better(g, c, best, dst, up)) {
+                best = g;
+                dst = c;
+            }
+        }
+        vv.N[v] = final_choice<VER>(dst, src, up);
+        put_sin<BT>(A, v, sin, hacc[2 * h] + hacc[2 * h + 1]);
+        hacc[2 * h] = 0;
+        hacc[2 * h + 1] = 0;
+    }
+    flush_acc(A.acc, A.integral, sin, 0);
+}
+
+template <int CS, int WK, int PREC, int VER, int BT>
+size_t cluster_smem() {
+    return (size_t)kClusterSlots * ((kIntg<WK> ? sizeof(uint64_t) : sizeof(uint32_t) + sizeof(double)) + sizeof(uint16_t));
+}
+
+template <int CS, int WK, int PREC, int VER, int BT>
+cudaLaunchConfig_t cluster_config(size_t smem, unsigned grid, cudaStream_t s, cudaLaunchAttribute *attr) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid, 1, 1);
+    cfg.blockDim = dim3(kClusterThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = CS;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+// Maximum co-resident clusters of a cluster kernel (0 when the shape cannot run).
+template <int CS, int WK, int PREC, int VER, int BT>
+int cluster_capacity() {
+    static int cap = -1;
+    if (cap >= 0) return cap;
+    auto kern = lm_cluster_kernel<CS, WK, PREC, VER, BT>;
+    const size_t smem = cluster_smem<CS, WK, PREC, VER, BT>();
+    MG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (CS > 8) MG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = cluster_config<CS, WK, PREC, VER, BT>(smem, CS * 148, nullptr, attr);
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, (void *)kern, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    cap = n;
+    return cap;
+}
+
+template <int CS, int WK, int PREC, int VER, int BT>
+void launch_cluster(const LMArgs &A, const uint32_t *verts, uint32_t count, cudaStream_t s) {
+    auto kern = lm_cluster_kernel<CS, WK, PREC, VER, BT>;
+    const size_t smem = cluster_smem<CS, WK, PREC, VER, BT>();
+    int cap = cluster_capacity<CS, WK, PREC, VER, BT>();
+    MG_CHECK(cap > 0, MG_ERR_UNSUPPORTED, "cluster shape cannot be scheduled on this device");
+    unsigned clusters = (unsigned)std::min<uint64_t>(count, (uint64_t)cap);
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = cluster_config<CS, WK, PREC, VER, BT>(smem, clusters * CS, s, attr);
+    MG_CUDA(cudaLaunchKernelEx(&cfg, kern, A, verts, count));
+    MG_LAUNCH_CHECK();
+}
+
+template <int WK, int PREC, int VER, int BT>
+void launch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, const LMArgs &A, cudaStream_t s) {
+    const Bins &B = lvl.bins;
+    // fork: heavy path on its own stream, the tile and hash bins on others
+    MG_CUDA(cudaEventRecord(ws.ev_fork, s));
+    for (int q = 0; q < 3; q++) MG_CUDA(cudaStreamWaitEvent(ws.streams[q], ws.ev_fork, 0));
+    cudaStream_t sh = ws.streams[0], sm = ws.streams[1], st = ws.streams[2];
+    // heavy tiers, largest clusters first
+    if (lvl.tier_off[5] > lvl.tier_off[4])
+        launch_cluster<16, WK, PREC, VER, BT>(A, ws.h_tier.get() + lvl.tier_off[4], lvl.tier_off[5] - lvl.tier_off[4], sh);
+    if (lvl.tier_off[4] > lvl.tier_off[3])
+        launch_cluster<8, WK, PREC, VER, BT>(A, ws.h_tier.get() + lvl.tier_off[3], lvl.tier_off[4] - lvl.tier_off[3], sh);
+    if (lvl.tier_off[3] > lvl.tier_off[2])
+        launch_cluster<4, WK, PREC, VER, BT>(A, ws.h_tier.get() + lvl.tier_off[2], lvl.tier_off[3] - lvl.tier_off[2], sh);
+    if (lvl.tier_off[2] > lvl.tier_off[1])
+        launch_cluster<2, WK, PREC, VER, BT>(A, ws.h_tier.get() + lvl.tier_off[1], lvl.tier_off[2] - lvl.tier_off[1], sh);
+    if (lvl.tier_off[1] > lvl.tier_off[0])
+        launch_cluster<1, WK, PREC, VER, BT>(A, ws.h_tier.get() + lvl.tier_off[0], lvl.tier_off[1] - lvl.tier_off[0], sm);
+    if (lvl.giants > 0) {
+        const uint32_t H = lvl.giants;
+        const uint32_t *hv = ws.h_tier.get() + lvl.tier_off[kTiers - 1];
+        heavy_insert_kernel<WK, VER, BT><<<lvl.ins_items, kHeavyThreads, 0, sh>>>(
+            A, hv, H, ws.h_ins.get(), ws.h_toff.get(), ws.h_tsize.get(), ws.h_keys.get(), ws.h_vals.get(),
+            ws.h_acc.get());
+        MG_LAUNCH_CHECK();
+        heavy_eval_kernel<PREC, BT><<<lvl.eval_items, kHeavyThreads, 0, sh>>>(
+            A, hv, H, ws.h_eval.get(), ws.h_toff.get(), ws.h_tsize.get(), ws.h_keys.get(), ws.h_vals.get(),
+            ws.h_acc.get(), ws.h_best.get());
+        MG_LAUNCH_CHECK();
+        heavy_final_kernel<PREC, VER, BT><<<(unsigned)ceil_div(H, 256), 256, 0, sh>>>(A, hv, H, ws.h_eval.get(),
+                                                                                  ws.h_acc.get(), ws.h_best.get());
+        MG_LAUNCH_CHECK();
+    }
+    using V = typename ValT<WK>::type;
+    auto hash_launch = [&](auto kern, int slots, int gpb, int block, int bin, cudaStream_t str) {
+        if (B.size[bin] == 0) return;
+        size_t smem = (size_t)slots * gpb * (sizeof(uint32_t) + sizeof(V) + sizeof(uint16_t) / 2);
+        MG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(B.size[bin], gpb), 148ull * 64);
+        kern<<<grid, block, smem, str>>>(A, B.offset[bin], B.size[bin]);
+        MG_LAUNCH_CHECK();
+    };
+    hash_launch(lm_hash_kernel<512, 8192, WK, PREC, VER, 512, BT>, 8192, 1, 512, 8, sm);
+    hash_launch(lm_hash_kernel<256, 4096, WK, PREC, VER, 256, BT>, 4096, 1, 256, 7, sm);
+    hash_launch(lm_hash_kernel<128, 1024, WK, PREC, VER, 128, BT>, 1024, 1, 128, 6, sm);
+    hash_launch(lm_hash_kernel<32, 256, WK, PREC, VER, 256, BT>, 256, 8, 256, 5, st);
+    auto tile_launch = [&](auto kern, int T, int bin, cudaStream_t str) {
+        if (B.size[bin] == 0) return;
+        uint64_t groups_per_block = 256 / T;
+        unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(B.size[bin], groups_per_block), 148ull * 32);
+        kern<<<grid, 256, 0, str>>>(A, B.offset[bin], B.size[bin]);
+        MG_LAUNCH_CHECK();
+    };
+    tile_launch(lm_tile_kernel<32, WK, PREC, VER, BT>, 32, 4, st);
+    tile_launch(lm_tile_kernel<16, WK, PREC, VER, BT>, 16, 3, st);
+    tile_launch(lm_tile_kernel<8, WK, PREC, VER, BT>, 8, 2, st);
+    tile_launch(lm_tile_kernel<4, WK, PREC, VER, BT>, 4, 1, st);
+    tile_launch(lm_tile_kernel<2, WK, PREC, VER, BT>, 2, 0, st);
+    for (int q = 0; q < 3; q++) {
+        MG_CUDA(cudaEventRecord(ws.ev_join[q], ws.streams[q]));
+        MG_CUDA(cudaStreamWaitEvent(s, ws.ev_join[q], 0));
+    }
+}
+
+// Weight kind / precision / version dispatch of one sweep.
+template <int BT>
+void dispatch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p,
+                    const LMArgs &A, cudaStream_t s) {
+    MG_CHECK(p.version == 1 || p.version == 2, MG_ERR_INVALID, "version must be 0, 1 or 2");
+    // integral graphs accumulate in integer table slots
+    const int wk = p.integral ? (g.wk == WK_F32 ? (int)WK_F32I : g.wk == WK_F64 ? (int)WK_F64I : g.wk) : g.wk;
+#define MG_SWEEP_CASE(WKV, PRECV)                                                                  \
+    if (wk == WKV && p.precision == PRECV) {                                                       \
+        if (p.version == 1) launch_sweep<WKV, PRECV, 1, BT>(g, lvl, ws, A, s);                     \
+        else launch_sweep<WKV, PRECV, 2, BT>(g, lvl, ws, A, s);                                    \
+        return;                                                                                    \
+    }
+    MG_SWEEP_CASE(WK_UNIT, MG_PREC_FP64)
+    MG_SWEEP_CASE(WK_F32I, MG_PREC_FP64)
+    MG_SWEEP_CASE(WK_F64I, MG_PREC_FP64)
+    MG_SWEEP_CASE(WK_F32, MG_PREC_FP64)
+    MG_SWEEP_CASE(WK_F64, MG_PREC_FP64)
+    MG_SWEEP_CASE(WK_UNIT, MG_PREC_INT64)
+    MG_SWEEP_CASE(WK_F32I, MG_PREC_INT64)
+    MG_SWEEP_CASE(WK_F64I, MG_PREC_INT64)
+    MG_SWEEP_CASE(WK_UNIT, MG_PREC_FP32)
+    MG_SWEEP_CASE(WK_F32I, MG_PREC_FP32)
+    MG_SWEEP_CASE(WK_F64I, MG_PREC_FP32)
+    MG_SWEEP_CASE(WK_F32, MG_PREC_FP32)
+    MG_SWEEP_CASE(WK_F64, MG_PREC_FP32)
+#undef MG_SWEEP_CASE
+    throw Error(MG_ERR_INVALID, "unknown weight kind or precision");
+}
+
+}  // namespace lmk
+}  // namespace mg

@@ -39,3 +39,28 @@ def test_null_arguments_fail_cleanly(mg):
     assert lib.mg_result_destroy(None) != 0
     assert lib.mg_init(None, None) != 0
     assert lib.mg_last_error(None)
+
+
+def test_batch_sbm_parameter_draw(mg):
+    """Host-side draw of a batch's SBM parameters: deterministic, inside the ranges."""
+    a = mg.draw_sbm_params(4096, seed=4)
+    b = mg.draw_sbm_params(4096, seed=4)
+    assert a == b
+    assert a != mg.draw_sbm_params(4096, seed=5)
+    n = [p["n"] for p in a]
+    assert min(n) >= 1000 and max(n) <= 200000
+    # log-uniform: the median sits near the geometric mean of the range
+    assert 10000 < sorted(n)[len(n) // 2] < 20000
+    for p in a:
+        assert 4 <= p["blocks"] <= min(256, p["n"])
+        assert 8.0 <= p["mean_degree"] <= 32.0 and 0.7 <= p["intra_frac"] <= 0.9
+    assert len({p["seed"] for p in a}) == 4096
+    lib = mg.lib()
+    assert lib.mg_batch_draw_sbm_params(1, 10, 5, 4, 256, 8.0, 32.0, 0.7, 0.9, 1, None) != 0
+
+
+def test_batch_null_arguments(mg):
+    lib = mg.lib()
+    assert lib.mg_batch_destroy(None) != 0
+    assert lib.mg_batch_result_destroy(None) != 0
+    assert lib.mg_batch_run(None, None, 0, None) != 0
