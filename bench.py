@@ -9,6 +9,21 @@ summed over ranks and divided by the slowest rank's time.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
+On one GPU the line also carries "batched": the batched form on 4,096 seeded
+SBM graphs (vertex counts log-uniform in [1k, 200k], 4-256 planted
+communities, mean degree uniform in [8, 32], 70-90% intra-community edges,
+unit weights) -- graphs/s of one batched run against the graphs/s of a loop
+of single-graph runs over a systematic sample of the same graphs, and a check
+that every sampled graph got the same modularity both ways.
+
+It also carries "serving": a Poisson stream of Louvain jobs (default 200
+requests/s for 60 s; half SBM, half R-MAT with edge factor 16 and the
+R-MAT-24 probabilities; vertex counts log-uniform in [1k, 8M]) submitted to
+the continuous-batching server (4 slots sharing a 150 GB HBM budget):
+offered and served jobs/s and the submit-to-done latency percentiles of the
+jobs completed within the window (jobs still queued at its end are reported
+with their count and age).
+
 --impl reference times the reference's Louvain logic on the host cores (the
 CPU oracle port under OpenMP, all host threads): each step is one phase-0
 sweep (local move + sigma update + modularity) over the same graph.
@@ -43,6 +58,12 @@ def parse():
     ap.add_argument("--scale", type=int, default=RMAT["scale"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batch-graphs", type=int, default=4096)
+    ap.add_argument("--batch-steps", type=int, default=2)
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-seconds", type=float, default=60.0)
     return ap.parse_args()
 
 
@@ -207,6 +228,123 @@ def run_reference(args, world, rank, local, pg):
     return line
 
 
+BATCH = dict(n_range=(1000, 200000), blocks_range=(4, 256), deg_range=(8.0, 32.0), intra_range=(0.7, 0.9), seed=4)
+
+
+def run_batched(mg, ctx, args):
+    """Batched form vs a per-graph loop of the plain path on the same GPU."""
+    params = mg.draw_sbm_params(args.batch_graphs, **BATCH)
+    b = ctx.batch_generate_sbm(params)
+    info = b.info()
+    b.run(assignments=False)  # warm-up
+    walls, devs, runs = [], [], []
+    for _ in range(max(args.batch_steps, 1)):
+        t0 = time.perf_counter()
+        r = b.run(assignments=False)
+        walls.append(time.perf_counter() - t0)
+        devs.append(r["seconds_total"])
+        runs.append(r)
+    q = runs[-1]["graphs"]["modularity"]
+    b.close()
+    # per-graph loop over a systematic sample (every step-th graph)
+    step = max(1, args.batch_graphs // 64)
+    loop_wall, loop_dev, same, k = 0.0, 0.0, 0, 0
+    for i in range(0, args.batch_graphs, step):
+        p = params[i]
+        g = ctx.generate_sbm(p["n"], p["blocks"], p["mean_degree"], p["intra_frac"], p["seed"])
+        g.louvain()  # first run of a size may grow buffers; time the second
+        t0 = time.perf_counter()
+        r = g.louvain()
+        loop_wall += time.perf_counter() - t0
+        loop_dev += r["seconds_total"]
+        same += int(r["modularity"] == q[i])
+        k += 1
+        g.close()
+    wall = statistics.median(walls)
+    return {
+        "workload": f"{args.batch_graphs} SBM graphs, one batched run", "graphs": args.batch_graphs,
+        "vertices": info["n"], "directed_entries": info["nnz"], "params": BATCH,
+        "graphs_per_s": args.batch_graphs / wall, "run_s": wall, "device_s": statistics.median(devs),
+        "sweeps": runs[-1]["sweeps"], "levels": runs[-1]["levels"],
+        "gpu_launches": runs[-1]["kernel_launches"],
+        "loop_graphs_per_s": k / loop_wall, "loop_sample": k, "loop_device_graphs_per_s": k / loop_dev,
+        "speedup_vs_loop": (args.batch_graphs / wall) / (k / loop_wall),
+        "modularity_equal": f"{same}/{k}", "mean_modularity": float(q.mean()),
+        "mode": "CUDA-graph iteration loop (MG_BATCH_GRAPHS)",
+    }
+
+
+SERVE = dict(n_range=(1000, 8_000_000), blocks_range=(4, 256), deg_range=(8.0, 32.0), intra_range=(0.7, 0.9),
+             rmat_edge_factor=16, abc=(0.57, 0.19, 0.19), slots=4, budget=150 * 10**9, seed=5)
+
+
+def serve_jobs(mg, count, seed):
+    """Job stream of the serving workload: alternating SBM / R-MAT, vertex
+    counts log-uniform (R-MAT: the nearest power of two)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    lo, hi = SERVE["n_range"]
+    jobs = []
+    for i in range(count):
+        v = float(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+        if i % 2 == 0:
+            n = int(round(v))
+            blocks = int(rng.integers(SERVE["blocks_range"][0], min(SERVE["blocks_range"][1], n) + 1))
+            jobs.append(mg.gen_params("sbm", n=n, blocks=blocks, mean_degree=float(rng.uniform(*SERVE["deg_range"])),
+                                      intra_frac=float(rng.uniform(*SERVE["intra_range"])), seed=1000 + i))
+        else:
+            scale = int(min(23, max(10, round(np.log2(v)))))
+            a, b, c = SERVE["abc"]
+            jobs.append(mg.gen_params("rmat", scale=scale, edge_factor=SERVE["rmat_edge_factor"], a=a, b=b, c=c,
+                                      seed=1000 + i))
+    return jobs
+
+
+def run_serving(mg, args, local):
+    """Poisson arrivals into the continuous-batching server for a fixed window."""
+    import numpy as np
+
+    rng = np.random.default_rng(SERVE["seed"])
+    expected = int(args.serve_rate * args.serve_seconds * 1.2) + 16
+    jobs = serve_jobs(mg, expected, SERVE["seed"])
+    gaps = rng.exponential(1.0 / args.serve_rate, expected)
+    srv = mg.Server(device=local, slots=SERVE["slots"], hbm_budget_bytes=SERVE["budget"])
+    ids, t_sub = [], []
+    t0 = time.perf_counter()
+    t_next = 0.0
+    for i in range(expected):
+        t_next += gaps[i]
+        if t_next >= args.serve_seconds:
+            break
+        delay = t0 + t_next - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit(jobs[i]))
+    window = max(time.perf_counter() - t0, args.serve_seconds)
+    if window > time.perf_counter() - t0:
+        time.sleep(window - (time.perf_counter() - t0))
+    st = srv.stats()
+    infos = [srv.poll(j) for j in ids]
+    done = [i for i in infos if i["state"] == mg.JOB_DONE]
+    lat = np.array([i["finished_s"] - i["submitted_s"] for i in done]) if done else np.zeros(1)
+    now = st["elapsed_s"]
+    waiting = [now - i["submitted_s"] for i in infos if i["state"] in (mg.JOB_QUEUED, mg.JOB_RUNNING)]
+    edges = sum(i["nnz"] for i in done)
+    t_stop = time.perf_counter()
+    srv.stop()  # cancels the queue, lets running batches finish
+    return {
+        "workload": f"Poisson {args.serve_rate:g} req/s for {args.serve_seconds:g} s, SBM + R-MAT, "
+                    f"vertices log-uniform in [1k, 8M]", "params": {k: v for k, v in SERVE.items()},
+        "offered_jobs_per_s": len(ids) / window, "served_jobs_per_s": len(done) / window,
+        "submitted": len(ids), "completed": len(done), "failed": st["failed"],
+        "unfinished": len(waiting), "unfinished_max_age_s": max(waiting) if waiting else 0.0,
+        "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+        "mean_latency_s": float(lat.mean()), "served_edges_per_s": edges / window,
+        "batches": st["batches"], "stop_s": time.perf_counter() - t_stop,
+    }
+
+
 def run_engine(args, world, rank, local, pg):
     mg = importlib.import_module("mg-alphagcd_b200")
     ctx = mg.Context(local)
@@ -262,6 +400,14 @@ def run_engine(args, world, rank, local, pg):
                "sample": f"one phase-0 sweep (local move + sigma update + modularity) over the same graph, "
                          f"{ct_:.1f} s on {threads} threads"}
         del csr
+    batched = serving = None
+    if world == 1 and not args.no_batched:
+        g.close()
+        batched = run_batched(mg, ctx, args)
+    if world == 1 and not args.no_serving:
+        g.close()
+        ctx.close()  # the server's slots take the HBM budget
+        serving = run_serving(mg, args, local)
     if rank != 0:
         return None
     line = {
@@ -288,6 +434,8 @@ def run_engine(args, world, rank, local, pg):
                 "d2h_bytes_per_step": 4 * info["n"]},
         "clocks": clk,
         "gpu_launches": int(sum(r["kernel_launches"] for r in runs)),
+        "batched": batched,
+        "serving": serving,
     }
     return line
 

@@ -225,6 +225,23 @@ mg_status mg_batch_draw_sbm_params(uint32_t graphs, uint32_t n_min, uint32_t n_m
                                    double intra_max, uint64_t seed, mg_sbm_params *out);
 /* Generate graph g of the batch exactly as mg_graph_generate_sbm(params[g]). */
 mg_status mg_batch_generate_sbm(mg_ctx *ctx, uint32_t graphs, const mg_sbm_params *params, mg_batch **out);
+
+/* one seeded generated graph: an SBM (mg_graph_generate_sbm) or an R-MAT
+ * graph (mg_graph_generate_rmat) */
+enum { MG_GEN_SBM = 0, MG_GEN_RMAT = 1 };
+typedef struct {
+    int kind;            /* MG_GEN_* */
+    uint32_t n;          /* SBM: vertices */
+    uint32_t blocks;     /* SBM: planted communities */
+    double mean_degree;  /* SBM */
+    double intra_frac;   /* SBM */
+    int scale;           /* R-MAT: 2^scale vertices */
+    int edge_factor;     /* R-MAT: pairs per vertex */
+    double a, b, c;      /* R-MAT quadrant probabilities */
+    uint64_t seed;
+} mg_gen_params;
+/* Generate graph g of the batch exactly as the single-graph generator of its kind. */
+mg_status mg_batch_generate(mg_ctx *ctx, uint32_t graphs, const mg_gen_params *params, mg_batch **out);
 /* Pack host graphs: graph g owns vertices [vertex_offsets[g], vertex_offsets[g+1])
  * of the packed rows; row v's entries are [offsets[v], offsets[v+1]) (64-bit,
  * packed over all graphs); cols hold graph-local vertex ids.  weights as in
@@ -260,6 +277,74 @@ mg_status mg_batch_result_graph(const mg_batch_result *r, uint32_t g, mg_batch_g
 /* final community (dense, graph-local) of every vertex of graph g: n_g entries */
 mg_status mg_batch_result_assignment(const mg_batch_result *r, uint32_t g, uint32_t *out);
 mg_status mg_batch_result_destroy(mg_batch_result *r);
+
+/* ---- serving ---------------------------------------------------------------------
+ * No reference counterpart.  A server admits Louvain jobs from any number of
+ * host threads and runs them with continuous batching: `slots` worker
+ * threads, each with its own context (streams and workspaces) and an equal
+ * share of the HBM budget, take the queued jobs in arrival order as soon as
+ * they are free, pack as many as fit their share into one batch
+ * (mg_batch_run) and run it; batches of different slots overlap on the GPU.
+ * A job is done as soon as its own graph finishes inside its batch.  Each
+ * job's result equals mg_louvain_run on its graph alone (bit for bit on
+ * integral weights).  All mg_serve_* calls are thread-safe. */
+typedef struct mg_server mg_server;
+
+typedef struct {
+    int device;
+    int slots;                 /* batches in flight (default 4) */
+    size_t hbm_budget_bytes;   /* shared equally by the slots (default 150e9) */
+    uint32_t max_batch_jobs;   /* jobs per batch at most (default 4096) */
+    int batch_flags;           /* MG_BATCH_* (default MG_BATCH_GRAPHS) */
+} mg_serve_opts;
+
+enum { MG_JOB_QUEUED = 0, MG_JOB_RUNNING = 1, MG_JOB_DONE = 2, MG_JOB_FAILED = 3, MG_JOB_CANCELLED = 4 };
+
+typedef struct {
+    int state;                     /* MG_JOB_* */
+    mg_status status;              /* of a failed job */
+    mg_batch_graph_summary graph;  /* result of a done job */
+    double submitted_s;            /* times in seconds since the server started */
+    double started_s;
+    double finished_s;
+    uint64_t batch;                /* batch the job ran in (1, 2, ...) */
+    uint32_t batch_jobs;           /* jobs in that batch */
+} mg_job_info;
+
+typedef struct {
+    uint64_t submitted, completed, failed, cancelled, queued, running;
+    uint64_t batches;
+    double elapsed_s;              /* since the server started */
+    double jobs_per_s;             /* completed / elapsed */
+    double p50_latency_s, p99_latency_s, mean_latency_s, max_latency_s; /* submit -> done */
+    size_t budget_bytes;
+    size_t reserved_bytes;         /* estimates of the jobs running now */
+} mg_serve_counters;
+
+/* Start the worker slots (opts may be NULL for the defaults). */
+mg_status mg_serve_start(const mg_serve_opts *opts, mg_server **out);
+/* Queue a generated graph; opts NULL = defaults; keep_assignment: keep the
+ * final assignment for mg_serve_assignment.  Jobs larger than one slot's
+ * budget are refused with MG_ERR_OOM. */
+mg_status mg_serve_submit(mg_server *s, const mg_gen_params *job, const mg_run_opts *opts, int keep_assignment,
+                          uint64_t *id);
+/* Queue a host CSR graph (copied at submit; arguments as mg_graph_from_csr). */
+mg_status mg_serve_submit_csr(mg_server *s, uint32_t n, const uint64_t *offsets, const uint32_t *cols,
+                              const void *weights, int weight_type, const mg_run_opts *opts, int keep_assignment,
+                              uint64_t *id);
+mg_status mg_serve_poll(mg_server *s, uint64_t id, mg_job_info *info);
+/* Wait until the job is done, failed or cancelled; MG_ERR_TIMEOUT after timeout_s. */
+mg_status mg_serve_wait(mg_server *s, uint64_t id, double timeout_s, mg_job_info *info);
+/* The kept assignment of a done job (graph.n entries). */
+mg_status mg_serve_assignment(mg_server *s, uint64_t id, uint32_t *out);
+/* Cancel a queued job (running jobs finish). */
+mg_status mg_serve_cancel(mg_server *s, uint64_t id);
+/* Forget a finished job. */
+mg_status mg_serve_release(mg_server *s, uint64_t id);
+mg_status mg_serve_stats(mg_server *s, mg_serve_counters *out);
+const char *mg_serve_last_error(mg_server *s);
+/* Cancel the queued jobs, wait for the running batches, stop the workers. */
+mg_status mg_serve_stop(mg_server *s);
 
 #ifdef __cplusplus
 }

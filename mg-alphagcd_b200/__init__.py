@@ -73,7 +73,35 @@ class _BatchGraph(ct.Structure):
                 ("levels", ct.c_int), ("iterations", ct.c_uint64), ("communities", ct.c_uint32)]
 
 
+class GenParams(ct.Structure):
+    _fields_ = [("kind", ct.c_int), ("n", ct.c_uint32), ("blocks", ct.c_uint32), ("mean_degree", ct.c_double),
+                ("intra_frac", ct.c_double), ("scale", ct.c_int), ("edge_factor", ct.c_int), ("a", ct.c_double),
+                ("b", ct.c_double), ("c", ct.c_double), ("seed", ct.c_uint64)]
+
+
+class _ServeOpts(ct.Structure):
+    _fields_ = [("device", ct.c_int), ("slots", ct.c_int), ("hbm_budget_bytes", ct.c_size_t),
+                ("max_batch_jobs", ct.c_uint32), ("batch_flags", ct.c_int)]
+
+
+class _JobInfo(ct.Structure):
+    _fields_ = [("state", ct.c_int), ("status", ct.c_int), ("graph", _BatchGraph), ("submitted_s", ct.c_double),
+                ("started_s", ct.c_double), ("finished_s", ct.c_double), ("batch", ct.c_uint64),
+                ("batch_jobs", ct.c_uint32)]
+
+
+class _ServeCounters(ct.Structure):
+    _fields_ = [("submitted", ct.c_uint64), ("completed", ct.c_uint64), ("failed", ct.c_uint64),
+                ("cancelled", ct.c_uint64), ("queued", ct.c_uint64), ("running", ct.c_uint64),
+                ("batches", ct.c_uint64), ("elapsed_s", ct.c_double), ("jobs_per_s", ct.c_double),
+                ("p50_latency_s", ct.c_double), ("p99_latency_s", ct.c_double), ("mean_latency_s", ct.c_double),
+                ("max_latency_s", ct.c_double), ("budget_bytes", ct.c_size_t), ("reserved_bytes", ct.c_size_t)]
+
+
 BATCH_GRAPHS = 1
+GEN_SBM, GEN_RMAT = 0, 1
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED = 0, 1, 2, 3, 4
+MG_ERR_TIMEOUT = 7
 
 EXPORTED = [
     "mg_status_string", "mg_version", "mg_init", "mg_destroy", "mg_last_error", "mg_graph_from_csr",
@@ -83,7 +111,9 @@ EXPORTED = [
     "mg_result_level_sizes", "mg_result_trace", "mg_result_destroy", "mg_local_move_noalloc",
     "mg_batch_draw_sbm_params", "mg_batch_generate_sbm", "mg_batch_from_csr", "mg_batch_info",
     "mg_batch_graph_info", "mg_batch_destroy", "mg_batch_run", "mg_batch_result_summary", "mg_batch_result_graph",
-    "mg_batch_result_assignment", "mg_batch_result_destroy",
+    "mg_batch_result_assignment", "mg_batch_result_destroy", "mg_batch_generate", "mg_serve_start",
+    "mg_serve_submit", "mg_serve_submit_csr", "mg_serve_poll", "mg_serve_wait", "mg_serve_assignment",
+    "mg_serve_cancel", "mg_serve_release", "mg_serve_stats", "mg_serve_last_error", "mg_serve_stop",
 ]
 
 
@@ -135,6 +165,19 @@ def lib():
     L.mg_batch_result_graph.argtypes = [vp, u32, ct.POINTER(_BatchGraph)]
     L.mg_batch_result_assignment.argtypes = [vp, u32, vp]
     L.mg_batch_result_destroy.argtypes = [vp]
+    L.mg_batch_generate.argtypes = [vp, u32, vp, pp]
+    L.mg_serve_start.argtypes = [ct.POINTER(_ServeOpts), pp]
+    L.mg_serve_submit.argtypes = [vp, ct.POINTER(GenParams), ct.POINTER(_RunOpts), i32, ct.POINTER(u64)]
+    L.mg_serve_submit_csr.argtypes = [vp, u32, vp, vp, vp, i32, ct.POINTER(_RunOpts), i32, ct.POINTER(u64)]
+    L.mg_serve_poll.argtypes = [vp, u64, ct.POINTER(_JobInfo)]
+    L.mg_serve_wait.argtypes = [vp, u64, dbl, ct.POINTER(_JobInfo)]
+    L.mg_serve_assignment.argtypes = [vp, u64, vp]
+    L.mg_serve_cancel.argtypes = [vp, u64]
+    L.mg_serve_release.argtypes = [vp, u64]
+    L.mg_serve_stats.argtypes = [vp, ct.POINTER(_ServeCounters)]
+    L.mg_serve_last_error.restype = ct.c_char_p
+    L.mg_serve_last_error.argtypes = [vp]
+    L.mg_serve_stop.argtypes = [vp]
     _lib = L
     return L
 
@@ -230,6 +273,14 @@ class Context:
                    "mg_batch_generate_sbm")
         return Batch(self, h)
 
+    def batch_generate(self, params) -> "Batch":
+        """Batch of generated graphs [GenParams, ...] (SBM and R-MAT mixed)."""
+        arr = (GenParams * len(params))(*params)
+        h = ct.c_void_p()
+        self.check(lib().mg_batch_generate(self.h, len(params), ct.cast(arr, ct.c_void_p), ct.byref(h)),
+                   "mg_batch_generate")
+        return Batch(self, h)
+
     def batch_from_csr(self, graphs) -> "Batch":
         """Pack host graphs [(n, offsets, cols, weights|None), ...] (local ids)."""
         G = len(graphs)
@@ -259,6 +310,103 @@ class Context:
         self.check(lib().mg_batch_from_csr(self.h, G, _p(voff), _p(off), _p(col), _p(w), wt, ct.byref(h)),
                    "mg_batch_from_csr")
         return Batch(self, h)
+
+
+def gen_params(kind: str, **kw) -> GenParams:
+    """A generated job: gen_params("sbm", n=, blocks=, mean_degree=, intra_frac=, seed=) or
+    gen_params("rmat", scale=, edge_factor=16, a=.57, b=.19, c=.19, seed=)."""
+    if kind == "sbm":
+        return GenParams(GEN_SBM, kw["n"], kw["blocks"], kw.get("mean_degree", 16.0), kw.get("intra_frac", 0.8),
+                         0, 0, 0.0, 0.0, 0.0, kw.get("seed", 1))
+    return GenParams(GEN_RMAT, 0, 0, 0.0, 0.0, kw["scale"], kw.get("edge_factor", 16), kw.get("a", 0.57),
+                     kw.get("b", 0.19), kw.get("c", 0.19), kw.get("seed", 2))
+
+
+class Server:
+    """Continuous-batching Louvain server (mg_serve_*): thread-safe submit / wait."""
+
+    def __init__(self, device: int = 0, slots: int = 4, hbm_budget_bytes: int = 150 * 10**9,
+                 max_batch_jobs: int = 4096, graphs: bool = True):
+        self.h = ct.c_void_p()
+        o = _ServeOpts(device, slots, hbm_budget_bytes, max_batch_jobs, BATCH_GRAPHS if graphs else 0)
+        st = lib().mg_serve_start(ct.byref(o), ct.byref(self.h))
+        if st != MG_OK:
+            raise MGError(st, lib().mg_last_error(None).decode())
+
+    def _check(self, st, what):
+        if st != MG_OK:
+            raise MGError(st, f"{what}: {lib().mg_serve_last_error(self.h).decode()}")
+
+    def submit(self, job: GenParams, keep_assignment: bool = False, version: int = 2, threshold: float = 1e-6,
+               max_phases: int = 1000, precision: str = "fp64") -> int:
+        o = _RunOpts(version, threshold, max_phases, _PREC[precision], 0)
+        jid = ct.c_uint64()
+        self._check(lib().mg_serve_submit(self.h, ct.byref(job), ct.byref(o), int(keep_assignment), ct.byref(jid)),
+                    "mg_serve_submit")
+        return jid.value
+
+    def submit_csr(self, n, offsets, cols, weights=None, keep_assignment: bool = False, **run) -> int:
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        col = np.ascontiguousarray(cols, dtype=np.uint32)
+        w, wt = (None, WEIGHT_UNIT) if weights is None else (np.ascontiguousarray(weights, np.float64), WEIGHT_F64)
+        o = _RunOpts(run.get("version", 2), run.get("threshold", 1e-6), run.get("max_phases", 1000),
+                     _PREC[run.get("precision", "fp64")], 0)
+        jid = ct.c_uint64()
+        self._check(lib().mg_serve_submit_csr(self.h, n, _p(off), _p(col), _p(w), wt, ct.byref(o),
+                                              int(keep_assignment), ct.byref(jid)), "mg_serve_submit_csr")
+        return jid.value
+
+    @staticmethod
+    def _info(i: _JobInfo) -> dict:
+        d = {f: getattr(i, f) for f, _ in _JobInfo._fields_ if f != "graph"}
+        d.update({f: getattr(i.graph, f) for f, _ in _BatchGraph._fields_})
+        return d
+
+    def poll(self, jid: int) -> dict:
+        i = _JobInfo()
+        self._check(lib().mg_serve_poll(self.h, jid, ct.byref(i)), "mg_serve_poll")
+        return self._info(i)
+
+    def wait(self, jid: int, timeout: float = 600.0) -> dict:
+        i = _JobInfo()
+        st = lib().mg_serve_wait(self.h, jid, timeout, ct.byref(i))
+        if st == MG_ERR_TIMEOUT:
+            raise TimeoutError(f"job {jid} not done after {timeout} s")
+        self._check(st, "mg_serve_wait")
+        return self._info(i)
+
+    def assignment(self, jid: int, n: int) -> np.ndarray:
+        a = np.zeros(max(n, 1), np.uint32)
+        self._check(lib().mg_serve_assignment(self.h, jid, _p(a)), "mg_serve_assignment")
+        return a[:n]
+
+    def cancel(self, jid: int) -> bool:
+        return lib().mg_serve_cancel(self.h, jid) == MG_OK
+
+    def release(self, jid: int) -> bool:
+        return lib().mg_serve_release(self.h, jid) == MG_OK
+
+    def stats(self) -> dict:
+        c = _ServeCounters()
+        self._check(lib().mg_serve_stats(self.h, ct.byref(c)), "mg_serve_stats")
+        return {f: getattr(c, f) for f, _ in _ServeCounters._fields_}
+
+    def stop(self):
+        if self.h:
+            lib().mg_serve_stop(self.h)
+            self.h = ct.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.stop()
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass
 
 
 def draw_sbm_params(graphs: int, n_range=(1000, 200000), blocks_range=(4, 256), deg_range=(8.0, 32.0),

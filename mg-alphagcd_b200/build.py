@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CXXFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
             "-ccbin", "/usr/bin/g++", "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]
 SOURCES = ["primitives.cu", "bins.cu", "local_move.cu", "local_move_batch.cu", "coarsen.cu", "graph.cu",
-           "louvain.cu", "batch.cu", "capi.cu",
+           "louvain.cu", "batch.cu", "serve.cu", "capi.cu",
            "mtx.cpp", "noalloc.cu"]
 LIB = os.path.join(HERE, "libmgagcd.so")
 CLI = os.path.join(HERE, "MG_GCD")

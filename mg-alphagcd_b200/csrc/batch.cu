@@ -466,7 +466,7 @@ void build_phase_graph(mg_ctx *ctx, mg_batch *b, const Body &B, cudaStream_t s, 
 
 }  // namespace
 
-void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &res) {
+void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &res, const GraphDoneFn *done) {
     mg_ctx *ctx = b->ctx;
     ctx_prepare(ctx);
     cudaStream_t s = ctx->stream;
@@ -526,8 +526,7 @@ void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &re
     unsigned long long *iters = W.iters.ensure(G);
     BatchCtrl *ctrl = W.ctrl.ensure(1);
     if (!W.h_ctrl) MG_CUDA(cudaMallocHost(&W.h_ctrl, sizeof(BatchCtrl)));
-    DBuf<uint8_t> dalive;
-    uint8_t *alive_d = dalive.ensure(G);
+    uint8_t *alive_d = W.alive.ensure(G);
     {
         std::vector<GainK> hk(G);
         for (uint32_t g = 0; g < G; g++) hk[g] = gain_constants(alive[g] ? b->mass[g] : 1.0);
@@ -542,6 +541,18 @@ void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &re
     std::vector<uint32_t> hgoff(b->voff.begin(), b->voff.end()), hgoff_new(G + 1);
     std::vector<double> hq(G), Qh(G, 0.0), Qold(G, -1.0);
     std::vector<int> phases(G, 0);
+    // results handed out early (done callback): graphs without edges now,
+    // the others when their run ends
+    std::vector<unsigned long long> hit(G);
+    std::vector<uint32_t> tmp_assign;
+    if (done) {
+        for (uint32_t g = 0; g < G; g++) {
+            if (alive[g]) continue;
+            tmp_assign.resize(res.per[g].n);
+            for (uint32_t v = 0; v < res.per[g].n; v++) tmp_assign[v] = v;
+            (*done)(g, res.per[g], tmp_assign.data());
+        }
+    }
 
     const unsigned long long launches0 = g_kernel_launches;
     W.h_ctrl->sweeps = 0;
@@ -668,6 +679,7 @@ void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &re
         MG_CUDA(cudaMemcpyAsync(hgoff_new.data(), goff_new, sizeof(uint32_t) * (G + 1), cudaMemcpyDeviceToHost, s));
         MG_CUDA(cudaStreamSynchronize(s));
         any_alive = 0;
+        std::vector<uint32_t> fin;
         for (uint32_t g = 0; g < G; g++) {
             if (!alive[g]) continue;
             Qh[g] = hq[g];
@@ -675,8 +687,28 @@ void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &re
             if (Qh[g] - Qold[g] <= thr) {
                 alive[g] = 0;
                 phases[g] = phase;
+                fin.push_back(g);
             } else {
                 any_alive = 1;
+            }
+        }
+        if (done && !fin.empty()) {
+            // the composed assignment of a finished graph is final; its local
+            // ids are offsets from the graph's first community
+            MG_CUDA(cudaMemcpyAsync(hit.data(), iters, sizeof(unsigned long long) * G, cudaMemcpyDeviceToHost, s));
+            for (uint32_t g : fin)
+                if (res.per[g].n)
+                    MG_CUDA(cudaMemcpyAsync(res.assignment.data() + b->voff[g], assign + b->voff[g],
+                                            sizeof(uint32_t) * res.per[g].n, cudaMemcpyDeviceToHost, s));
+            MG_CUDA(cudaStreamSynchronize(s));
+            for (uint32_t g : fin) {
+                uint32_t *a = res.assignment.data() + b->voff[g];
+                for (uint32_t v = 0; v < res.per[g].n; v++) a[v] -= hgoff_new[g];
+                mg_batch_graph_summary P = res.per[g];
+                P.modularity = Qh[g];
+                P.phases = phases[g];
+                P.iterations = hit[g];
+                (*done)(g, P, a);
             }
         }
         if (!any_alive) {
@@ -706,7 +738,6 @@ void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &re
         MG_LAUNCH_CHECK();
     }
     MG_CUDA(cudaEventRecord(ctx->ev[3], s));
-    std::vector<unsigned long long> hit(G);
     MG_CUDA(cudaMemcpyAsync(hit.data(), iters, sizeof(unsigned long long) * G, cudaMemcpyDeviceToHost, s));
     MG_CUDA(cudaMemcpyAsync(W.h_ctrl, ctrl, sizeof(BatchCtrl), cudaMemcpyDeviceToHost, s));
     if (n0 > 0)
@@ -725,6 +756,9 @@ void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &re
         P.iterations = hit[g];
         S.iterations += (int)hit[g];
     }
+    if (done)  // graphs stopped by max_phases
+        for (uint32_t g = 0; g < G; g++)
+            if (alive[g]) (*done)(g, res.per[g], res.assignment.data() + b->voff[g]);
 }
 
 }  // namespace mg

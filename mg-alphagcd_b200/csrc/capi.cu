@@ -517,11 +517,37 @@ static mg_status batch_new(mg_ctx *ctx, uint32_t graphs, mg_batch **out, mg_batc
     return MG_OK;
 }
 
+mg_status mg_batch_generate(mg_ctx *ctx, uint32_t graphs, const mg_gen_params *params, mg_batch **out) {
+    mg_batch *b = nullptr;
+    mg_status st = batch_new(ctx, graphs, out, &b);
+    if (st != MG_OK) return st;
+    st = guarded(ctx, [&] { batch_generate(b, params); });
+    if (st != MG_OK) {
+        delete b;
+        return st;
+    }
+    *out = b;
+    return MG_OK;
+}
+
 mg_status mg_batch_generate_sbm(mg_ctx *ctx, uint32_t graphs, const mg_sbm_params *params, mg_batch **out) {
     mg_batch *b = nullptr;
     mg_status st = batch_new(ctx, graphs, out, &b);
     if (st != MG_OK) return st;
-    st = guarded(ctx, [&] { batch_generate_sbm(b, params); });
+    st = guarded(ctx, [&] {
+        MG_CHECK(params != nullptr, MG_ERR_INVALID, "batch: params is NULL");
+        std::vector<mg_gen_params> gp(graphs);
+        for (uint32_t g = 0; g < graphs; g++) {
+            gp[g] = mg_gen_params{};
+            gp[g].kind = MG_GEN_SBM;
+            gp[g].n = params[g].n;
+            gp[g].blocks = params[g].blocks;
+            gp[g].mean_degree = params[g].mean_degree;
+            gp[g].intra_frac = params[g].intra_frac;
+            gp[g].seed = params[g].seed;
+        }
+        batch_generate(b, gp.data());
+    });
     if (st != MG_OK) {
         delete b;
         return st;

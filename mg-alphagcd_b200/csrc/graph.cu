@@ -9,30 +9,36 @@ namespace mg {
 
 namespace {
 
+// pair k of a seeded R-MAT graph of 2^scale vertices: one quadrant choice per
+// bit level, two levels per 64-bit random word
+__device__ __forceinline__ void rmat_pair(int scale, uint64_t t1, uint64_t t2, uint64_t t3, uint64_t key, uint64_t k,
+                                          uint32_t &u, uint32_t &v) {
+    const int words = (scale + 1) / 2;
+    uint32_t uu = 0, vv = 0;
+    for (int wi = 0; wi < words; wi++) {
+        uint64_t r = rng_at(key, k * (uint64_t)words + (uint64_t)wi);
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            int l = 2 * wi + h;
+            if (l >= scale) break;
+            uint64_t x = h ? (r >> 32) : (r & 0xFFFFFFFFull);
+            uint32_t bu, bv;
+            if (x < t1) { bu = 0; bv = 0; }
+            else if (x < t2) { bu = 0; bv = 1; }
+            else if (x < t3) { bu = 1; bv = 0; }
+            else { bu = 1; bv = 1; }
+            uu |= bu << (scale - 1 - l);
+            vv |= bv << (scale - 1 - l);
+        }
+    }
+    u = uu;
+    v = vv;
+}
+
 __global__ void rmat_pairs_kernel(int scale, uint64_t m, uint64_t t1, uint64_t t2, uint64_t t3, uint64_t key,
                                   uint32_t *u, uint32_t *v) {
-    const int words = (scale + 1) / 2;
-    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (uint64_t)gridDim.x * blockDim.x) {
-        uint32_t uu = 0, vv = 0;
-        for (int wi = 0; wi < words; wi++) {
-            uint64_t r = rng_at(key, k * (uint64_t)words + (uint64_t)wi);
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                int l = 2 * wi + h;
-                if (l >= scale) break;
-                uint64_t x = h ? (r >> 32) : (r & 0xFFFFFFFFull);
-                uint32_t bu, bv;
-                if (x < t1) { bu = 0; bv = 0; }
-                else if (x < t2) { bu = 0; bv = 1; }
-                else if (x < t3) { bu = 1; bv = 0; }
-                else { bu = 1; bv = 1; }
-                uu |= bu << (scale - 1 - l);
-                vv |= bv << (scale - 1 - l);
-            }
-        }
-        u[k] = uu;
-        v[k] = vv;
-    }
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (uint64_t)gridDim.x * blockDim.x)
+        rmat_pair(scale, t1, t2, t3, key, k, u[k], v[k]);
 }
 
 // pair k of a seeded SBM: the first min_ pairs join two vertices of one block,
@@ -65,16 +71,19 @@ __global__ void sbm_pairs_kernel(uint32_t n, uint32_t blocks, uint64_t min_, uin
         sbm_pair(n, blocks, min_, kin, kout, k, u[k], v[k]);
 }
 
-// per-graph parameters of a batch of SBMs
-struct SbmDev {
-    uint32_t n, blocks, vbase, pad;
-    uint64_t min_, kin, kout, pbase;  // pbase: first pair of the graph
+// per-graph parameters of a generated batch
+struct GenDev {
+    uint32_t kind, n, blocks, vbase;  // SBM: vertices, blocks; first vertex in the union
+    int scale, pad;                   // R-MAT
+    uint64_t min_, kin, kout;         // SBM: intra pairs, stream keys / R-MAT: key in kin
+    uint64_t t1, t2, t3;              // R-MAT quadrant thresholds
+    uint64_t pbase;                   // first pair of the graph
 };
 
 // all pairs of all graphs of a batch; graph of pair k by binary search over
 // the pair bases (G + 1 entries)
-__global__ void sbm_batch_pairs_kernel(const SbmDev *gp, const uint64_t *pbase, uint32_t G, uint64_t M, uint32_t *u,
-                                       uint32_t *v) {
+__global__ void batch_pairs_kernel(const GenDev *gp, const uint64_t *pbase, uint32_t G, uint64_t M, uint32_t *u,
+                                   uint32_t *v) {
     for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M; k += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t lo = 0, hi = G;  // last graph with pbase <= k
         while (hi - lo > 1) {
@@ -82,9 +91,10 @@ __global__ void sbm_batch_pairs_kernel(const SbmDev *gp, const uint64_t *pbase, 
             if (pbase[mid] <= k) lo = mid;
             else hi = mid;
         }
-        const SbmDev p = gp[lo];
+        const GenDev &p = gp[lo];
         uint32_t a, b;
-        sbm_pair(p.n, p.blocks, p.min_, p.kin, p.kout, k - p.pbase, a, b);
+        if (p.kind == MG_GEN_RMAT) rmat_pair(p.scale, p.t1, p.t2, p.t3, p.kin, k - p.pbase, a, b);
+        else sbm_pair(p.n, p.blocks, p.min_, p.kin, p.kout, k - p.pbase, a, b);
         u[k] = p.vbase + a;
         v[k] = p.vbase + b;
     }
@@ -367,63 +377,93 @@ __global__ void gather_u32_kernel(const uint32_t *src, const uint32_t *idx, uint
 static void batch_entry_offsets(mg_batch *b) {
     cudaStream_t s = b->ctx->stream;
     const uint32_t G = b->graphs;
-    DBuf<uint32_t> idx, out;
-    MG_CUDA(cudaMemcpyAsync(idx.ensure(G + 1), b->voff.data(), sizeof(uint32_t) * (G + 1), cudaMemcpyHostToDevice, s));
-    gather_u32_kernel<<<(unsigned)ceil_div(G + 1, 256), 256, 0, s>>>(b->u.off.get(), idx.get(), G + 1,
-                                                                     out.ensure(G + 1));
+    uint32_t *idx = b->work.small.ensure(2 * (G + 1)), *out = idx + G + 1;
+    MG_CUDA(cudaMemcpyAsync(idx, b->voff.data(), sizeof(uint32_t) * (G + 1), cudaMemcpyHostToDevice, s));
+    gather_u32_kernel<<<(unsigned)ceil_div(G + 1, 256), 256, 0, s>>>(b->u.off.get(), idx, G + 1, out);
     MG_LAUNCH_CHECK();
     std::vector<uint32_t> h(G + 1);
-    MG_CUDA(cudaMemcpyAsync(h.data(), out.get(), sizeof(uint32_t) * (G + 1), cudaMemcpyDeviceToHost, s));
+    MG_CUDA(cudaMemcpyAsync(h.data(), out, sizeof(uint32_t) * (G + 1), cudaMemcpyDeviceToHost, s));
     MG_CUDA(cudaStreamSynchronize(s));
     b->eoff.assign(h.begin(), h.end());
 }
 
-void batch_generate_sbm(mg_batch *b, const mg_sbm_params *params) {
+void batch_generate(mg_batch *b, const mg_gen_params *params) {
     const uint32_t G = b->graphs;
     MG_CHECK(G >= 1 && params != nullptr, MG_ERR_INVALID, "batch: need at least one graph and its parameters");
-    std::vector<SbmDev> gp(G);
+    std::vector<GenDev> gp(G);
     std::vector<uint64_t> pbase(G + 1, 0);
     b->voff.assign(G + 1, 0);
     uint64_t nv = 0, M = 0;
     for (uint32_t g = 0; g < G; g++) {
-        const mg_sbm_params &p = params[g];
-        MG_CHECK(p.blocks >= 1 && p.n >= p.blocks, MG_ERR_INVALID, "sbm: need 1 <= blocks <= n");
-        // pair counts exactly as graph_generate_sbm
-        const double din = p.mean_degree * p.intra_frac;
-        const double dout = p.mean_degree - din;
-        const uint64_t min_ = (uint64_t)std::llround((double)p.n * din / 2.0);
-        const uint64_t mout = p.blocks > 1 ? (uint64_t)std::llround((double)p.n * dout / 2.0) : 0;
-        gp[g].n = p.n;
-        gp[g].blocks = p.blocks;
-        gp[g].vbase = (uint32_t)nv;
-        gp[g].min_ = min_;
-        gp[g].kin = rng_key(p.seed, 0x53424d31ull);
-        gp[g].kout = rng_key(p.seed, 0x53424d32ull);
-        gp[g].pbase = M;
+        const mg_gen_params &p = params[g];
+        GenDev &d = gp[g];
+        d = GenDev{};
+        d.kind = (uint32_t)p.kind;
+        uint64_t m = 0;
+        if (p.kind == MG_GEN_SBM) {
+            MG_CHECK(p.blocks >= 1 && p.n >= p.blocks, MG_ERR_INVALID, "sbm: need 1 <= blocks <= n");
+            // pair counts exactly as graph_generate_sbm
+            const double din = p.mean_degree * p.intra_frac;
+            const double dout = p.mean_degree - din;
+            const uint64_t min_ = (uint64_t)std::llround((double)p.n * din / 2.0);
+            const uint64_t mout = p.blocks > 1 ? (uint64_t)std::llround((double)p.n * dout / 2.0) : 0;
+            d.n = p.n;
+            d.blocks = p.blocks;
+            d.min_ = min_;
+            d.kin = rng_key(p.seed, 0x53424d31ull);
+            d.kout = rng_key(p.seed, 0x53424d32ull);
+            m = min_ + mout;
+        } else if (p.kind == MG_GEN_RMAT) {
+            // as graph_generate_rmat
+            MG_CHECK(p.scale >= 1 && p.scale <= 31 && p.edge_factor >= 1, MG_ERR_INVALID, "rmat: bad scale or edge factor");
+            MG_CHECK(p.a >= 0 && p.b >= 0 && p.c >= 0 && p.a + p.b + p.c <= 1.0, MG_ERR_INVALID,
+                     "rmat: bad probabilities");
+            d.n = 1u << p.scale;
+            d.scale = p.scale;
+            d.t1 = (uint64_t)(p.a * 4294967296.0);
+            d.t2 = (uint64_t)((p.a + p.b) * 4294967296.0);
+            d.t3 = (uint64_t)((p.a + p.b + p.c) * 4294967296.0);
+            d.kin = rng_key(p.seed, 0x524d4154ull);
+            m = (uint64_t)p.edge_factor << p.scale;
+        } else {
+            throw Error(MG_ERR_INVALID, "batch: unknown generator kind");
+        }
+        d.vbase = (uint32_t)nv;
+        d.pbase = M;
         pbase[g] = M;
         b->voff[g] = (uint32_t)nv;
-        nv += p.n;
-        M += min_ + mout;
+        nv += d.n;
+        M += m;
         MG_CHECK(nv < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "batch: more than 2^32-1 vertices in total");
         MG_CHECK(2 * M < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "batch: more than 2^32-1 directed entries in total");
     }
     pbase[G] = M;
     b->voff[G] = (uint32_t)nv;
     cudaStream_t s = b->ctx->stream;
-    DBuf<uint32_t> u, v;
-    u.ensure(M + 1);
-    v.ensure(M + 1);
+    BatchWork &W = b->work;
+    uint32_t *u = W.pu.ensure(M + 1), *v = W.pv.ensure(M + 1);
     if (M > 0) {
-        DBuf<SbmDev> dgp;
-        DBuf<uint64_t> dpb;
-        MG_CUDA(cudaMemcpyAsync(dgp.ensure(G), gp.data(), sizeof(SbmDev) * G, cudaMemcpyHostToDevice, s));
-        MG_CUDA(cudaMemcpyAsync(dpb.ensure(G + 1), pbase.data(), sizeof(uint64_t) * (G + 1), cudaMemcpyHostToDevice,
-                                s));
-        sbm_batch_pairs_kernel<<<148 * 16, 256, 0, s>>>(dgp.get(), dpb.get(), G, M, u.get(), v.get());
+        GenDev *dgp = (GenDev *)W.gen.ensure(sizeof(GenDev) * G);
+        uint64_t *dpb = W.pbase.ensure(G + 1);
+        MG_CUDA(cudaMemcpyAsync(dgp, gp.data(), sizeof(GenDev) * G, cudaMemcpyHostToDevice, s));
+        MG_CUDA(cudaMemcpyAsync(dpb, pbase.data(), sizeof(uint64_t) * (G + 1), cudaMemcpyHostToDevice, s));
+        batch_pairs_kernel<<<148 * 16, 256, 0, s>>>(dgp, dpb, G, M, u, v);
         MG_LAUNCH_CHECK();
-        MG_CUDA(cudaStreamSynchronize(s));
     }
-    finish_generated(&b->u, (uint32_t)nv, M, u, v);
+    // symmetric deduplicated CSR of the union; the union's previous buffers
+    // are kept in W.built for the next batch
+    csr_from_device_pairs((uint32_t)nv, M, u, v, W.built, b->ctx->cws, s);
+    mg_graph *ug = &b->u;
+    ug->n = (uint32_t)nv;
+    ug->nnz = W.built.nnz;
+    std::swap(ug->off.p, W.built.off.p);
+    std::swap(ug->off.cap, W.built.off.cap);
+    std::swap(ug->col.p, W.built.col.p);
+    std::swap(ug->col.cap, W.built.col.cap);
+    ug->wk = WK_UNIT;
+    ug->mass = (double)ug->nnz;
+    ug->integral = ug->nnz < 4294967296ull;
+    MG_CUDA(cudaStreamSynchronize(s));
     batch_entry_offsets(b);
     b->mass.resize(G);
     b->integral.resize(G);
@@ -482,19 +522,16 @@ void batch_from_host_csr(mg_batch *b, const uint64_t *voff, const uint64_t *offs
     u->n = (uint32_t)n;
     u->nnz = nnz;
     {
-        DBuf<uint64_t> off64;
-        DBuf<uint32_t> dvoff;
-        DBuf<int> bad;
-        uint64_t *d64 = off64.ensure(n + 1);
-        int *dbad = bad.ensure(1);
+        BatchWork &W = b->work;
+        uint64_t *d64 = W.off64.ensure(n + 1);
+        int *dbad = W.bad.ensure(1);
+        uint32_t *dvoff = W.small.ensure(2 * (G + 1));
         MG_CUDA(cudaMemsetAsync(dbad, 0, sizeof(int), s));
         MG_CUDA(cudaMemcpyAsync(d64, offsets, sizeof(uint64_t) * (n + 1), cudaMemcpyHostToDevice, s));
-        MG_CUDA(cudaMemcpyAsync(dvoff.ensure(G + 1), b->voff.data(), sizeof(uint32_t) * (G + 1),
-                                cudaMemcpyHostToDevice, s));
+        MG_CUDA(cudaMemcpyAsync(dvoff, b->voff.data(), sizeof(uint32_t) * (G + 1), cudaMemcpyHostToDevice, s));
         uint32_t *dcol = u->col.ensure(nnz + 1);
         if (nnz) MG_CUDA(cudaMemcpyAsync(dcol, cols, sizeof(uint32_t) * nnz, cudaMemcpyHostToDevice, s));
-        batch_rows_kernel<<<148 * 16, 256, 0, s>>>(d64, (uint32_t)n, dvoff.get(), G, dcol, u->off.ensure(n + 1),
-                                                   dbad);
+        batch_rows_kernel<<<148 * 16, 256, 0, s>>>(d64, (uint32_t)n, dvoff, G, dcol, u->off.ensure(n + 1), dbad);
         MG_LAUNCH_CHECK();
         int hbad = 0;
         MG_CUDA(cudaMemcpyAsync(&hbad, dbad, sizeof(int), cudaMemcpyDeviceToHost, s));

@@ -2,6 +2,7 @@
 // mg_result) and the engine entry points the ABI calls.
 #pragma once
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -83,6 +84,14 @@ struct BatchWork {
     DBuf<GSum> sums;
     DBuf<BatchCtrl> ctrl;
     BatchCtrl *h_ctrl = nullptr;  // pinned
+    // construction and run scratch, kept so that a batch object reused for
+    // the next set of graphs allocates (and frees) nothing once warm
+    DBuf<uint32_t> pu, pv, small;
+    DBuf<uint64_t> off64, pbase;
+    DBuf<unsigned char> gen;
+    DBuf<int> bad;
+    DBuf<uint8_t> alive;
+    LevelGraph built;  // swapped with the union's buffers by the generator
     ~BatchWork();
 };
 }  // namespace mg
@@ -109,6 +118,8 @@ struct mg_batch_result {
 namespace mg {
 
 void ctx_prepare(mg_ctx *ctx);
+// error text for entry points that run without a context (mg_last_error(NULL))
+void set_orphan_error(const std::string &msg);
 // graph construction
 void graph_from_host_csr(mg_graph *g, uint32_t n, const uint64_t *offsets, const uint32_t *cols, const void *w,
                          int weight_type);
@@ -124,9 +135,12 @@ mg_status load_mtx_host(const char *path, uint32_t &n, std::vector<uint64_t> &of
 // Louvain
 void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result &res);
 // batched form
-void batch_generate_sbm(mg_batch *b, const mg_sbm_params *params);
+void batch_generate(mg_batch *b, const mg_gen_params *params);
 void batch_from_host_csr(mg_batch *b, const uint64_t *voff, const uint64_t *offsets, const uint32_t *cols,
                          const void *w, int weight_type);
-void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &res);
+// Called by batch_run, on its thread, as soon as graph g's result is final:
+// its summary and its graph-local assignment (n_g entries).
+using GraphDoneFn = std::function<void(uint32_t g, const mg_batch_graph_summary &sum, const uint32_t *assignment)>;
+void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &res, const GraphDoneFn *done = nullptr);
 
 }  // namespace mg

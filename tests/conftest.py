@@ -81,3 +81,9 @@ def boundary_degree_graph():
             u.append(i)
             v.append(n_centers + j)
     return n_centers + leaves, np.array(u), np.array(v)
+
+
+def cuda_available() -> bool:
+    import torch
+
+    return torch.cuda.is_available()
