@@ -196,6 +196,28 @@ mg_status mg_result_level_sizes(const mg_result *r, uint32_t *out, int max, int 
 mg_status mg_result_trace(const mg_result *r, double *rows4, int max_rows, int *count);
 mg_status mg_result_destroy(mg_result *r);
 
+/* ---- autotuner -------------------------------------------------------------------
+ * No reference counterpart (the reference's bin thresholds and kernel shapes
+ * are fixed, src/bin/BIN.cu:72-92).  The local move groups vertices in degree
+ * classes (class c: 2^(c-1) < degree <= 2^c) and works each class up to 4096
+ * with a kernel shape: T-lane tiles or shared-memory tables with 32 to 512
+ * threads per vertex.  Any shape whose table holds the class gives the same
+ * result, so the shape per class is picked by timing: the first sweep of a
+ * level times the candidate shapes of each class of at least 4096 vertices that
+ * is not yet in the context's table, and the fastest is stored (keyed by weight
+ * kind, precision, version, single / batched sweep, class and class size) and
+ * reused.  MG_TUNE_OFF uses the built-in shapes, MG_TUNE_CACHED the table
+ * without timing anything new, MG_TUNE_ON (default) also fills it. */
+enum { MG_TUNE_OFF = 0, MG_TUNE_CACHED = 1, MG_TUNE_ON = 2 };
+mg_status mg_tune_mode(mg_ctx *ctx, int mode);
+/* The table as text, one entry per line:
+ * "<weight kind> <precision> <version> <batched> <class> <size bucket> <shape> <microseconds>".
+ * *len receives the length; buf (capacity cap) may be NULL. */
+mg_status mg_tune_table(mg_ctx *ctx, char *buf, size_t cap, size_t *len);
+/* Save / load the table (same text). Loading merges into the context's table. */
+mg_status mg_tune_save(mg_ctx *ctx, const char *path);
+mg_status mg_tune_load(mg_ctx *ctx, const char *path);
+
 /* ---- batched form --------------------------------------------------------------
  * No reference counterpart: the reference runs one graph per process.  A batch
  * packs many independent graphs as one disjoint union on the device and runs

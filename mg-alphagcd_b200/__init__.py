@@ -114,7 +114,9 @@ EXPORTED = [
     "mg_batch_result_assignment", "mg_batch_result_destroy", "mg_batch_generate", "mg_serve_start",
     "mg_serve_submit", "mg_serve_submit_csr", "mg_serve_poll", "mg_serve_wait", "mg_serve_assignment",
     "mg_serve_cancel", "mg_serve_release", "mg_serve_stats", "mg_serve_last_error", "mg_serve_stop",
+    "mg_tune_mode", "mg_tune_table", "mg_tune_save", "mg_tune_load",
 ]
+TUNE_OFF, TUNE_CACHED, TUNE_ON = 0, 1, 2
 
 
 def lib():
@@ -166,6 +168,10 @@ def lib():
     L.mg_batch_result_assignment.argtypes = [vp, u32, vp]
     L.mg_batch_result_destroy.argtypes = [vp]
     L.mg_batch_generate.argtypes = [vp, u32, vp, pp]
+    L.mg_tune_mode.argtypes = [vp, i32]
+    L.mg_tune_table.argtypes = [vp, ct.c_char_p, ct.c_size_t, ct.POINTER(ct.c_size_t)]
+    L.mg_tune_save.argtypes = [vp, ct.c_char_p]
+    L.mg_tune_load.argtypes = [vp, ct.c_char_p]
     L.mg_serve_start.argtypes = [ct.POINTER(_ServeOpts), pp]
     L.mg_serve_submit.argtypes = [vp, ct.POINTER(GenParams), ct.POINTER(_RunOpts), i32, ct.POINTER(u64)]
     L.mg_serve_submit_csr.argtypes = [vp, u32, vp, vp, vp, i32, ct.POINTER(_RunOpts), i32, ct.POINTER(u64)]
@@ -262,6 +268,29 @@ class Context:
         nb = {0: 10, 1: 11, 2: 9}[scheme]
         return {"sizes": sizes[:nb], "offsets": boff[:nb], "perm": perm[:n], "max_degree": int(md.value)}
 
+
+    # ---- autotuner ------------------------------------------------------------
+    def tune_mode(self, mode: int):
+        """TUNE_OFF: built-in shapes; TUNE_CACHED: table only; TUNE_ON: also time new classes."""
+        self.check(lib().mg_tune_mode(self.h, mode), "mg_tune_mode")
+
+    def tune_table(self) -> list:
+        """Entries: (weight kind, precision, version, batched, class, size bucket, shape, microseconds)."""
+        n = ct.c_size_t()
+        self.check(lib().mg_tune_table(self.h, None, 0, ct.byref(n)), "mg_tune_table")
+        buf = ct.create_string_buffer(n.value + 1)
+        self.check(lib().mg_tune_table(self.h, buf, n.value + 1, ct.byref(n)), "mg_tune_table")
+        out = []
+        for line in buf.value.decode().splitlines():
+            f = line.split()
+            out.append(tuple(int(x) for x in f[:6]) + (f[6], float(f[7])))
+        return out
+
+    def tune_save(self, path: str):
+        self.check(lib().mg_tune_save(self.h, path.encode()), "mg_tune_save")
+
+    def tune_load(self, path: str):
+        self.check(lib().mg_tune_load(self.h, path.encode()), "mg_tune_load")
 
     # ---- batches ------------------------------------------------------------
     def batch_generate_sbm(self, params) -> "Batch":

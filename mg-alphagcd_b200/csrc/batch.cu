@@ -22,7 +22,7 @@
 //
 // Graphs converge after different numbers of sweeps, so a phase runs until its
 // slowest graph is done.  The sweeps therefore walk compacted lists of the
-// vertices of active graphs -- the degree-bin list (bins 0-8, in bin order)
+// vertices of active graphs -- the degree-class list (classes 0-12, in class order)
 // and the vertex list (id order) for the per-graph sums and sigma updates --
 // with the graph of every entry stored beside it.  The lists are rebuilt at the
 // start of a phase and whenever the vertices of active graphs fall to half of
@@ -324,7 +324,7 @@ __global__ void list_scatter_kernel(const uint32_t *list, const uint32_t *lgid, 
 }
 
 struct Idx12 {
-    uint32_t v[12];
+    uint32_t v[kLightClasses + 1];
 };
 __global__ void gather_idx_kernel(const uint32_t *pos, Idx12 idx, int cnt, uint32_t *out) {
     if ((int)threadIdx.x < cnt) out[threadIdx.x] = pos[idx.v[threadIdx.x]];
@@ -369,19 +369,22 @@ void rebuild_lists(mg_ctx *ctx, BatchWork &W, const MoveLevel &full, Lists &Ls, 
     const int nxt = from_level ? Ls.cur : Ls.cur ^ 1;
     const uint32_t *gid = W.gid.get(), *gword = W.gword.get();
     PrimWorkspace &pw = ctx->cws.prim;
-    // bins 0-8
+    // light classes (0-12); the heavy classes keep the level's own lists
     const Bins &src = from_level ? full.bins : Ls.lvl.bins;
-    uint32_t bounds[10], nb[10];
-    for (int b = 0; b < 9; b++) bounds[b] = src.offset[b];
-    const uint32_t L = src.offset[9];
+    uint32_t bounds[kLightClasses + 1], nb[kLightClasses + 1];
+    for (int b = 0; b < kLightClasses; b++) bounds[b] = src.offset[b];
+    const uint32_t L = src.offset[kLightClasses];
     compact_list(from_level ? ctx->mws.perm.get() : W.lperm[Ls.cur].get(), from_level ? nullptr : W.lpgid[Ls.cur].get(),
-                 gid, L, gword, W.lperm[nxt].get(), W.lpgid[nxt].get(), W, pw, s, bounds, 9, nb);
+                 gid, L, gword, W.lperm[nxt].get(), W.lpgid[nxt].get(), W, pw, s, bounds, kLightClasses, nb);
+    uint8_t shapes[kLightClasses];
+    for (int b = 0; b < kLightClasses; b++) shapes[b] = Ls.lvl.shape[b];
     Ls.lvl = full;
-    for (int b = 0; b < 9; b++) {
+    for (int b = 0; b < kLightClasses; b++) {
         Ls.lvl.bins.offset[b] = nb[b];
         Ls.lvl.bins.size[b] = nb[b + 1] - nb[b];
+        if (!from_level) Ls.lvl.shape[b] = shapes[b];  // a phase keeps the shapes tuned at its start
     }
-    Ls.lvl.bins.offset[9] = nb[9];
+    Ls.lvl.bins.offset[kLightClasses] = nb[kLightClasses];
     // vertices in id order
     uint32_t vb[1];
     compact_list(from_level ? nullptr : W.lvert[Ls.cur].get(), from_level ? nullptr : W.lvgid[Ls.cur].get(), gid,
@@ -621,6 +624,9 @@ void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &re
                                     cudaMemcpyHostToDevice, s));
         };
         use_lists();
+        // shapes of the light classes (autotuner): the timing runs write what
+        // the first sweep of the phase writes
+        move_tune_batch(cur, Ls.lvl, ctx->mws, sp, B.bs, k, sigma, s);
         // iterate until every graph has rejected a sweep.  The first sweep
         // after the lists change runs as plain launches (it also sets up the
         // launch shapes); the rest, with MG_BATCH_GRAPHS, as CUDA-graph loops.

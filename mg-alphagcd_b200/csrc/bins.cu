@@ -7,17 +7,29 @@
 // The reference scatters with atomics (order inside a bin unspecified,
 // BIN.cu:298-466); here the scatter ranks by vertex id, so every bin lists
 // its members in ascending order.
+//
+// Scheme 3 is the local-move sweep's own grouping (no reference counterpart;
+// the sweep's results do not depend on it): 19 degree classes,
+//   class 0: deg <= 1, class c (1..17): 2^(c-1) < deg <= 2^c, class 18: > 2^17,
+// so that the kernel shape of each class can be chosen freely (see
+// lm_kernels.cuh): classes 0-12 go to the tile / shared-memory hash shapes,
+// 13-17 to thread-block clusters of 1-16 CTAs, 18 to the global-table path.
 #include "engine.cuh"
 
 namespace mg {
 
-int bin_count(int scheme) { return scheme == 0 ? 10 : scheme == 1 ? 11 : 9; }
+int bin_count(int scheme) { return scheme == 0 ? 10 : scheme == 1 ? 11 : scheme == 2 ? 9 : kSweepClasses; }
 
 namespace {
 
 constexpr int kBinThreads = 1024;
 
 __device__ __forceinline__ int bin_of(int scheme, uint32_t d) {
+    if (scheme == 3) {
+        if (d <= 1) return 0;
+        const int c = 32 - __clz(d - 1);  // ceil(log2 d)
+        return c < kSweepClasses - 1 ? c : kSweepClasses - 1;
+    }
     if (scheme == 0) {
         if (d <= 32) return d <= 2 ? 0 : d <= 4 ? 1 : d <= 8 ? 2 : d <= 16 ? 3 : 4;
         return d <= 128 ? 5 : d <= 512 ? 6 : d <= 2048 ? 7 : d <= 4094 ? 8 : 9;
@@ -34,9 +46,9 @@ __device__ __forceinline__ int bin_of(int scheme, uint32_t d) {
 __global__ void __launch_bounds__(kBinThreads) bins_count_kernel(int scheme, int nb, uint32_t n, const uint32_t *off,
                                                                   uint32_t *counts, uint32_t blocks,
                                                                   uint32_t *max_deg) {
-    __shared__ uint32_t c[11];
+    __shared__ uint32_t c[kMaxBins];
     __shared__ uint32_t mx;
-    if (threadIdx.x < 11) c[threadIdx.x] = 0;
+    if (threadIdx.x < kMaxBins) c[threadIdx.x] = 0;
     if (threadIdx.x == 0) mx = 0;
     __syncthreads();
     uint32_t i = blockIdx.x * kBinThreads + threadIdx.x;
@@ -58,9 +70,9 @@ __global__ void __launch_bounds__(kBinThreads) bins_count_kernel(int scheme, int
 __global__ void __launch_bounds__(kBinThreads) bins_scatter_kernel(int scheme, uint32_t n, const uint32_t *off,
                                                                     const uint32_t *offs, uint32_t blocks,
                                                                     uint32_t *perm) {
-    __shared__ uint32_t wc[32][11];
+    __shared__ uint32_t wc[32][kMaxBins];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int t = threadIdx.x; t < 32 * 11; t += kBinThreads) (&wc[0][0])[t] = 0;
+    for (int t = threadIdx.x; t < 32 * kMaxBins; t += kBinThreads) (&wc[0][0])[t] = 0;
     __syncthreads();
     uint32_t i = blockIdx.x * kBinThreads + threadIdx.x;
     int b = -1;
@@ -69,7 +81,7 @@ __global__ void __launch_bounds__(kBinThreads) bins_scatter_kernel(int scheme, u
     uint32_t before = __popc(peers & ((1u << lane) - 1u));
     if (b >= 0 && before == 0) wc[warp][b] = __popc(peers);
     __syncthreads();
-    if (threadIdx.x < 11) {
+    if (threadIdx.x < kMaxBins) {
         uint32_t acc = 0;
         for (int w = 0; w < 32; w++) {
             uint32_t x = wc[w][threadIdx.x];
@@ -85,7 +97,7 @@ __global__ void __launch_bounds__(kBinThreads) bins_scatter_kernel(int scheme, u
 
 void compute_bins(int scheme, uint32_t n, const uint32_t *d_off, uint32_t *d_perm, Bins &out, cudaStream_t s,
                   PrimWorkspace &ws) {
-    MG_CHECK(scheme >= 0 && scheme <= 2, MG_ERR_INVALID, "bins: scheme must be 0, 1 or 2");
+    MG_CHECK(scheme >= 0 && scheme <= 3, MG_ERR_INVALID, "bins: scheme must be 0, 1, 2 or 3");
     int nb = bin_count(scheme);
     out = Bins();
     out.scheme = scheme;

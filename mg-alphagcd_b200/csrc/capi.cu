@@ -2,6 +2,7 @@
 // Every entry point catches engine errors and returns an mg_status; the
 // message of the last failure is kept on the context.
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <new>
 
@@ -262,6 +263,7 @@ mg_status mg_bins(mg_graph *g, int scheme, uint32_t *sizes, uint32_t *offsets, u
     mg_ctx *ctx = g->ctx;
     return guarded(ctx, [&] {
         ctx_prepare(ctx);
+        MG_CHECK(scheme >= 0 && scheme <= 2, MG_ERR_INVALID, "bins: scheme must be 0, 1 or 2");
         Bins b;
         uint32_t *d_perm = ctx->tmp32.ensure((size_t)g->n + 1);
         compute_bins(scheme, g->n, g->off.get(), d_perm, b, ctx->stream, ctx->mws.prim);
@@ -282,6 +284,7 @@ mg_status mg_bins_offsets(mg_ctx *ctx, int scheme, uint32_t n, const uint64_t *o
     if (!ctx || !offsets) return fail(ctx, MG_ERR_INVALID, "mg_bins_offsets: NULL argument");
     return guarded(ctx, [&] {
         ctx_prepare(ctx);
+        MG_CHECK(scheme >= 0 && scheme <= 2, MG_ERR_INVALID, "bins: scheme must be 0, 1 or 2");
         std::vector<uint32_t> o32((size_t)n + 1);
         for (uint32_t i = 0; i <= n; i++) {
             MG_CHECK(offsets[i] < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "offsets must be below 2^32-1");
@@ -474,6 +477,84 @@ mg_status mg_result_trace(const mg_result *r, double *rows4, int max_rows, int *
 mg_status mg_result_destroy(mg_result *r) {
     if (!r) return MG_ERR_INVALID;
     delete r;
+    return MG_OK;
+}
+
+// ---- autotuner ------------------------------------------------------------------
+
+namespace {
+std::string tune_text(const TuneTable &T) {
+    std::string out;
+    char line[160];
+    for (const auto &kv : T.entries) {
+        const uint32_t k = kv.first;
+        snprintf(line, sizeof line, "%u %u %u %u %u %u %s %.3f\n", k & 7u, (k >> 3) & 3u, (k >> 5) & 3u,
+                 (k >> 7) & 1u, (k >> 8) & 31u, k >> 13, shape_name(kv.second.shape), (double)kv.second.us);
+        out += line;
+    }
+    return out;
+}
+}  // namespace
+
+mg_status mg_tune_mode(mg_ctx *ctx, int mode) {
+    if (!ctx) return MG_ERR_INVALID;
+    if (mode < MG_TUNE_OFF || mode > MG_TUNE_ON) return fail(ctx, MG_ERR_INVALID, "mg_tune_mode: unknown mode");
+    ctx->mws.tune.mode = mode;
+    return MG_OK;
+}
+
+mg_status mg_tune_table(mg_ctx *ctx, char *buf, size_t cap, size_t *len) {
+    if (!ctx) return MG_ERR_INVALID;
+    return guarded(ctx, [&] {
+        const std::string t = tune_text(ctx->mws.tune);
+        if (len) *len = t.size();
+        if (buf && cap) {
+            const size_t n = t.size() < cap - 1 ? t.size() : cap - 1;
+            memcpy(buf, t.data(), n);
+            buf[n] = 0;
+        }
+    });
+}
+
+mg_status mg_tune_save(mg_ctx *ctx, const char *path) {
+    if (!ctx || !path) return MG_ERR_INVALID;
+    const std::string t = tune_text(ctx->mws.tune);
+    FILE *f = fopen(path, "w");
+    if (!f) return fail(ctx, MG_ERR_IO, std::string("mg_tune_save: cannot open ") + path);
+    const bool ok = fwrite(t.data(), 1, t.size(), f) == t.size();
+    fclose(f);
+    return ok ? MG_OK : fail(ctx, MG_ERR_IO, "mg_tune_save: write failed");
+}
+
+mg_status mg_tune_load(mg_ctx *ctx, const char *path) {
+    if (!ctx || !path) return MG_ERR_INVALID;
+    FILE *f = fopen(path, "r");
+    if (!f) return fail(ctx, MG_ERR_IO, std::string("mg_tune_load: cannot open ") + path);
+    char line[256];
+    std::map<uint32_t, TuneEntry> add;
+    mg_status st = MG_OK;
+    while (fgets(line, sizeof line, f)) {
+        unsigned wk, prec, ver, bt, cls, bucket;
+        char name[16];
+        double us;
+        if (sscanf(line, "%u %u %u %u %u %u %15s %lf", &wk, &prec, &ver, &bt, &cls, &bucket, name, &us) != 8 ||
+            wk > 4 || prec > 2 || ver > 2 || bt > 1 || cls >= (unsigned)kLightClasses || bucket > 31) {
+            st = MG_ERR_FORMAT;
+            break;
+        }
+        int sh = -1;
+        for (int i = 0; i < SH_COUNT; i++)
+            if (strcmp(name, shape_name(i)) == 0) sh = i;
+        if (sh < 0 || shape_capacity(sh) < (1u << cls)) {
+            st = MG_ERR_FORMAT;
+            break;
+        }
+        const uint32_t key = wk | prec << 3 | ver << 5 | bt << 7 | cls << 8 | bucket << 13;
+        add[key] = TuneEntry{(uint8_t)sh, (float)us};
+    }
+    fclose(f);
+    if (st != MG_OK) return fail(ctx, st, "mg_tune_load: malformed line");
+    for (const auto &kv : add) ctx->mws.tune.entries[kv.first] = kv.second;
     return MG_OK;
 }
 

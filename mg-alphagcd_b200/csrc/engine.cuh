@@ -1,6 +1,7 @@
 // engine.cuh -- internal interfaces between the engine's translation units.
 #pragma once
 
+#include <map>
 #include <vector>
 
 #include "common.cuh"
@@ -20,12 +21,17 @@ struct GraphView {
 };
 
 // Degree bins of one level.  Schemes: 0 = 10 local-move bins, 1 = 11
-// coarsen-symbolic bins, 2 = 9 coarsen-numeric bins.
+// coarsen-symbolic bins, 2 = 9 coarsen-numeric bins (the reference's three),
+// 3 = the sweep's 19 degree classes (class c holds 2^(c-1) < deg <= 2^c).
+constexpr int kMaxBins = 20;
+constexpr int kSweepScheme = 3, kSweepClasses = 19;
+constexpr int kLightClasses = 13;   // classes 0-12 (deg <= 4096): tile / hash shapes
+constexpr int kFirstHeavyClass = 13;
 struct Bins {
     int scheme = 0;
     int count = 0;
-    uint32_t size[11] = {0};
-    uint32_t offset[11] = {0};
+    uint32_t size[kMaxBins] = {0};
+    uint32_t offset[kMaxBins] = {0};
     uint32_t max_degree = 0;
 };
 
@@ -54,21 +60,66 @@ struct SweepAcc {
 constexpr int kClusterSlots = 16384;
 constexpr int kTiers = 6;
 
-// Per-level state of the local-move engine: bins and the heavy-vertex tables.
+// Kernel shapes of the light classes (0-12): T-lane tiles (deg <= T) and
+// shared-memory hash tables worked by GT threads per vertex.
+enum SweepShape : uint8_t {
+    SH_T2, SH_T4, SH_T8, SH_T16, SH_T32,  // tiles
+    SH_H32, SH_H64, SH_H128, SH_H256, SH_H512,  // hash, GT threads per vertex
+    SH_COUNT
+};
+// largest degree a shape serves
+inline uint32_t shape_capacity(int sh) {
+    switch (sh) {
+        case SH_T2: return 2;
+        case SH_T4: return 4;
+        case SH_T8: return 8;
+        case SH_T16: return 16;
+        case SH_T32: return 32;
+        case SH_H32: return 512;
+        case SH_H64: return 1024;
+        default: return 4096;
+    }
+}
+const char *shape_name(int sh);
+// the shapes used when nothing has been tuned
+int default_shape(int cls);
+
+// Per-level state of the local-move engine: degree classes, the shape of
+// every light class, and the heavy-vertex tables.
 struct MoveLevel {
-    Bins bins;
-    uint32_t heavy = 0;            // vertices in the last bin
-    uint32_t tier_off[kTiers + 1] = {0};  // heavy vertices by tier (ws.h_tier)
+    Bins bins;                     // sweep classes (scheme 3)
+    uint8_t shape[kLightClasses] = {0};
+    uint32_t heavy = 0;            // vertices of the heavy classes (13-18)
+    const uint32_t *heavy_list = nullptr;  // those vertices, by class (a range of the level's perm)
+    uint32_t tier_off[kTiers + 1] = {0};  // heavy vertices by tier (in heavy_list)
     uint32_t giants = 0;           // vertices on the global-table path
     uint32_t ins_items = 0;        // insert work items (vertex, edge chunk)
     uint32_t eval_items = 0;       // evaluate work items (vertex, slot chunk)
     uint64_t table_slots = 0;
 };
 
+// Autotuner table: the fastest shape of a light class, keyed by the kernel
+// weight kind, precision, version, single / batched sweep, class and the
+// class size (log2 bucket).  Filled by timing the candidate shapes of a class
+// on the level's first sweep; the sweep's results do not depend on the shapes.
+struct TuneEntry {
+    uint8_t shape;
+    float us;  // timed duration of the chosen shape
+};
+struct TuneTable {
+    int mode = MG_TUNE_ON;
+    std::map<uint32_t, TuneEntry> entries;
+    unsigned long long tuned = 0;  // classes tuned (timed) so far
+    static uint32_t key(int wk, int prec, int ver, int bt, int cls, uint32_t size) {
+        const uint32_t bucket = size ? 31u - (uint32_t)__builtin_clz(size) : 0u;
+        return (uint32_t)wk | (uint32_t)prec << 3 | (uint32_t)ver << 5 | (uint32_t)bt << 7 | (uint32_t)cls << 8 |
+               bucket << 13;
+    }
+};
+constexpr uint32_t kTuneMinVertices = 4096;  // smaller classes keep the default shape
+
 struct MoveWorkspace {
     DBuf<uint32_t> perm;
-    DBuf<uint32_t> h_tier;         // heavy vertices grouped by tier
-    DBuf<uint32_t> h_deg;          // degrees of the heavy vertices
     int max_cluster = 0;           // largest cluster size the device runs (8 or 16)
     // heavy-vertex global tables
     DBuf<uint64_t> h_toff;         // table offset per heavy vertex (H+1)
@@ -81,9 +132,12 @@ struct MoveWorkspace {
     DBuf<unsigned long long> h_best;  // per evaluate item: packed best (gain bits, id) x2
     DBuf<uint64_t> tmp64;
     DBuf<SweepAcc> acc;
+    DBuf<SweepAcc> tune_acc;       // sums of the autotuner's timing runs (discarded)
+    TuneTable tune;
     PrimWorkspace prim;
     cudaStream_t streams[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_join[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_tune[2] = {nullptr, nullptr};  // timing events of the autotuner
     ~MoveWorkspace();
     void init_streams();
 };
@@ -148,6 +202,13 @@ void move_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, con
 // the buffers and the gain constants, and sum_in goes to b.sinv.
 void move_sweep_batch(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p,
                       const BatchSweep &b, const double *k, const double *sigma, cudaStream_t s);
+// Shapes of the level's light classes from the tuning table; with MG_TUNE_ON,
+// classes missing from it are timed now with the sweep's arguments (P, N, k,
+// sigma as the next sweep will use them: the timing runs write the same N).
+void move_tune(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p, const uint32_t *P,
+               uint32_t *N, const double *k, const double *sigma, cudaStream_t s);
+void move_tune_batch(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p,
+                     const BatchSweep &b, const double *k, const double *sigma, cudaStream_t s);
 void sweep_reset_acc(MoveWorkspace &ws, cudaStream_t s);
 // sum of sigma^2 into ws.acc
 void sigma_sumsq(const double *sigma, uint32_t n, int integral, MoveWorkspace &ws, cudaStream_t s);

@@ -6,6 +6,9 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <mutex>
+#include <set>
+#include <utility>
 #include <vector>
 
 #include "engine.cuh"
@@ -296,7 +299,7 @@ __global__ void __launch_bounds__(256) lm_tile_kernel(LMArgs A, uint32_t bin_off
 }
 
 // ============================================================================
-// bins 5-8: GT threads per vertex, SLOTS-entry shared table
+// classes up to 4096: GT threads per vertex, shared-memory table
 // ============================================================================
 // table value type: 32-bit integer sums for integral weights, else double
 template <int WK>
@@ -308,49 +311,6 @@ template <int GT>
 __device__ __forceinline__ void group_sync() {
     if constexpr (GT == 32) __syncwarp();
     else __syncthreads();
-}
-
-// Two sums over a group of GT threads with one pair of barriers; results
-// valid in every thread.  red: 2 * 32 doubles.
-template <int GT>
-__device__ __forceinline__ void group_sum2(double &a, double &b, double *red) {
-    a = warp_sum(a);
-    b = warp_sum(b);
-    if constexpr (GT > 32) {
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        if (lane == 0) {
-            red[warp] = a;
-            red[32 + warp] = b;
-        }
-        __syncthreads();
-        double ta = 0, tb = 0;
-#pragma unroll
-        for (int w2 = 0; w2 < GT / 32; w2++) {
-            ta += red[w2];
-            tb += red[32 + w2];
-        }
-        __syncthreads();
-        a = ta;
-        b = tb;
-    }
-}
-
-// Sum over a group of GT threads; result valid in every thread.
-template <int GT>
-__device__ __forceinline__ double group_sum(double v, double *red) {
-    v = warp_sum(v);
-    if constexpr (GT == 32) {
-        return v;
-    } else {
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        if (lane == 0) red[warp] = v;
-        __syncthreads();
-        double t = 0;
-#pragma unroll
-        for (int w2 = 0; w2 < GT / 32; w2++) t += red[w2];
-        __syncthreads();
-        return t;
-    }
 }
 
 template <int GT, class G>
@@ -365,7 +325,10 @@ __device__ __forceinline__ void group_argmax(G &best, uint32_t &dst, int up, G *
         }
     }
     if constexpr (GT > 32) {
+        // the group's warps are [w0, w0 + GT/32) of the block (several groups
+        // may share a block)
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int w0 = (threadIdx.x / GT) * (GT / 32);
         if (lane == 0) {
             rg[warp] = best;
             rc[warp] = dst;
@@ -373,46 +336,20 @@ __device__ __forceinline__ void group_argmax(G &best, uint32_t &dst, int up, G *
         __syncthreads();
 #pragma unroll
         for (int w2 = 0; w2 < GT / 32; w2++) {
-            if (better(rg[w2], rc[w2], best, dst, up)) {
-                best = rg[w2];
-                dst = rc[w2];
+            if (better(rg[w0 + w2], rc[w0 + w2], best, dst, up)) {
+                best = rg[w0 + w2];
+                dst = rc[w0 + w2];
             }
         }
         __syncthreads();
     }
 }
 
-template <int X>
-struct Log2 {
-    static constexpr int value = 1 + Log2<X / 2>::value;
-};
-template <>
-struct Log2<1> {
-    static constexpr int value = 0;
-};
-
-template <int SLOTS>
-__device__ __forceinline__ uint32_t table_find_or_insert(uint32_t *keys, uint32_t c, int bits) {
-    const uint32_t mask = (1u << bits) - 1u;
-    uint32_t h = hash_slot(c, bits);
-    for (int p = 0; p < SLOTS; p++) {
-        uint32_t cur = ((volatile uint32_t *)keys)[h];
-        if (cur == c) return h;
-        if (cur == kEmpty) {
-            uint32_t prev = atomicCAS(keys + h, kEmpty, c);
-            if (prev == kEmpty || prev == c) return h;
-        }
-        h = (h + 1) & mask;
-    }
-    return kEmpty;  // unreachable: tables hold >= 2*deg slots
-}
-
 // table bits for a vertex of degree d: 2*d slots rounded up to a power of
-// two, at least 32, at most the group's table
-template <int SLOTS>
-__device__ __forceinline__ int table_bits(uint32_t d) {
+// two, at least 32, at most the group's table (2^max_bits slots)
+__device__ __forceinline__ int table_bits(uint32_t d, int max_bits) {
     const int want = d <= 16 ? 5 : 33 - __clz(2 * d - 1);
-    return want < Log2<SLOTS>::value ? want : Log2<SLOTS>::value;
+    return want < max_bits ? want : max_bits;
 }
 
 // weight of edge e as the table's value type: exact 32-bit integer for
@@ -433,30 +370,38 @@ __device__ __forceinline__ double v2d(V v) {
     else return v;
 }
 
-// Shared-memory hash table per group of GT threads.  Newly inserted slots are
-// appended to a per-table list, so the evaluation runs densely over the
-// distinct candidates only (and resets exactly those slots).
-template <int GT, int SLOTS, int WK, int PREC, int VER, int BLOCK, int BT>
-__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) lm_hash_kernel(LMArgs A, uint32_t bin_off, uint32_t bin_size) {
+constexpr uint64_t kEmpty64 = 0xFFFFFFFF00000000ull;
+
+// Shared-memory hash table of 2^slots_log2 slots per group of GT threads (a
+// power of two >= 2 * the largest degree of the launch, load <= 1/2): a key
+// array and a value array (32-bit integer sums for integral weights, doubles
+// otherwise).  Newly inserted slots are appended to a per-table list, so the
+// evaluation runs densely over the distinct candidates only (and resets
+// exactly those slots).
+template <int GT, int WK, int PREC, int VER, int BLOCK, int BT>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
+    lm_hash_kernel(LMArgs A, uint32_t bin_off, uint32_t bin_size, int slots_log2) {
     using G = typename Prec<PREC>::G;
     const int up = load_up<BT>(A);
     using V = typename ValT<WK>::type;
     constexpr int GPB = BLOCK / GT;
     constexpr int BATCH = 4;
     constexpr int EB = 4;
+    const uint32_t S = 1u << slots_log2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    uint32_t *keys_all = (uint32_t *)smem_raw;
-    V *vals_all = (V *)(smem_raw + sizeof(uint32_t) * SLOTS * GPB);
-    uint16_t *used_all = (uint16_t *)(smem_raw + (sizeof(uint32_t) + sizeof(V)) * SLOTS * GPB);
+    // values V [S * GPB] | keys u32 [S * GPB] | used u16 [S/2 * GPB]
+    V *vals_all = (V *)smem_raw;
+    uint32_t *keys_all = (uint32_t *)(smem_raw + sizeof(V) * S * GPB);
+    uint16_t *used_all = (uint16_t *)(smem_raw + (sizeof(V) + sizeof(uint32_t)) * S * GPB);
     __shared__ V acc_e[GPB], acc_s[GPB];
     __shared__ uint32_t cnt[GPB];
     __shared__ G red_g[32];
     __shared__ uint32_t red_c[32];
     const int g = threadIdx.x / GT, t = threadIdx.x % GT;
-    uint32_t *keys = keys_all + g * SLOTS;
-    V *vals = vals_all + g * SLOTS;
-    uint16_t *used = used_all + g * (SLOTS / 2);
-    for (int s2 = threadIdx.x; s2 < SLOTS * GPB; s2 += BLOCK) {
+    V *vals = vals_all + g * S;
+    uint32_t *keys = keys_all + g * S;
+    uint16_t *used = used_all + g * (S / 2);
+    for (uint32_t s2 = threadIdx.x; s2 < S * GPB; s2 += BLOCK) {
         keys_all[s2] = kEmpty;
         vals_all[s2] = V(0);
     }
@@ -485,7 +430,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) lm_hash_kernel(LMArgs A, 
             ki = A.k[i];
             a = A.sigma[src] - ki;  // issued early, consumed after the edge pass
         }
-        const int tb = table_bits<SLOTS>(hi - lo);
+        const int tb = table_bits(hi - lo, slots_log2);
+        const uint32_t mask = (1u << tb) - 1u;
         V e_part = V(0), s_part = V(0);
         for (uint32_t base = lo + t; base < hi; base += GT * BATCH) {
             uint32_t jj[BATCH], cc[BATCH];
@@ -503,24 +449,22 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) lm_hash_kernel(LMArgs A, 
                 if (jj[b] == kEmpty) continue;
                 const uint32_t c = cc[b];
                 if (c != src) {
-                    if (is_candidate<VER>(c, src, up)) {
-                        const uint32_t mask = (1u << tb) - 1u;
-                        uint32_t h = hash_slot(c, tb);
-                        for (int p = 0; p < SLOTS; p++) {
-                            uint32_t cur = ((volatile uint32_t *)keys)[h];
-                            if (cur == c) break;
-                            if (cur == kEmpty) {
-                                uint32_t prev = atomicCAS(keys + h, kEmpty, c);
-                                if (prev == kEmpty) {
-                                    used[atomicAdd(cnt + g, 1u)] = (uint16_t)h;
-                                    break;
-                                }
-                                if (prev == c) break;
+                    if (!is_candidate<VER>(c, src, up)) continue;
+                    uint32_t h = hash_slot(c, tb);
+                    for (uint32_t p = 0; p < S; p++) {
+                        const uint32_t cur = ((volatile uint32_t *)keys)[h];
+                        if (cur == c) break;
+                        if (cur == kEmpty) {
+                            const uint32_t prev = atomicCAS(keys + h, kEmpty, c);
+                            if (prev == kEmpty) {
+                                used[atomicAdd(cnt + g, 1u)] = (uint16_t)h;
+                                break;
                             }
-                            h = (h + 1) & mask;
+                            if (prev == c) break;
                         }
-                        atomicAdd(vals + h, ww[b]);
+                        h = (h + 1) & mask;
                     }
+                    atomicAdd(vals + h, ww[b]);
                 } else if (jj[b] != i) {
                     e_part += ww[b];
                 } else {
@@ -597,7 +541,6 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) lm_hash_kernel(LMArgs A, 
 // ============================================================================
 namespace cg = cooperative_groups;
 constexpr int kClusterThreads = 1024;  // one CTA per SM with a 16K-slot segment
-constexpr uint64_t kEmpty64 = 0xFFFFFFFF00000000ull;
 
 template <int CS>
 __device__ __forceinline__ void cluster_barrier() {
@@ -1064,27 +1007,87 @@ void launch_cluster(const LMArgs &A, const uint32_t *verts, uint32_t count, cuda
     MG_LAUNCH_CHECK();
 }
 
+// Bytes of dynamic shared memory of a hash launch with 2^slots_log2 slots per group.
+template <int WK>
+size_t hash_smem(int gpb, int slots_log2) {
+    const size_t per_slot = sizeof(typename ValT<WK>::type) + sizeof(uint32_t) + 1;
+    return ((size_t)1 << slots_log2) * (size_t)gpb * per_slot;
+}
+
+// The dynamic shared-memory limit of a kernel is a per-function setting, so it
+// is raised once per device to the largest table the kernel is launched with
+// (setting it per launch would race between threads launching different
+// table sizes).
+inline void raise_smem_limit(const void *kern, size_t smem) {
+    static std::mutex mu;
+    static std::set<std::pair<const void *, int>> done;  // (kernel, device)
+    int dev = 0;
+    MG_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count({kern, dev})) return;
+    MG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    done.insert({kern, dev});
+}
+
+// One light class (degrees <= 2^cls) with the given shape.
+template <int WK, int PREC, int VER, int BT>
+void launch_light(int shape, int cls, const LMArgs &A, uint32_t off, uint32_t size, cudaStream_t s) {
+    if (size == 0) return;
+    auto tile = [&](auto kern, int T) {
+        const uint64_t per_block = 256 / T;
+        const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(size, per_block), 148ull * 32);
+        kern<<<grid, 256, 0, s>>>(A, off, size);
+        MG_LAUNCH_CHECK();
+    };
+    auto hash = [&](auto kern, int gt, int block) {
+        const int gpb = block / gt;
+        const int sl = std::max(5, cls + 1);  // 2 * 2^cls slots, at least 32
+        const size_t smem = hash_smem<WK>(gpb, sl);
+        // the largest table of the shape: 2 * its capacity
+        int max_sl = 5;
+        while ((1u << max_sl) < 2 * shape_capacity(shape)) max_sl++;
+        raise_smem_limit((const void *)kern, hash_smem<WK>(gpb, max_sl));
+        const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(size, gpb), 148ull * 64);
+        kern<<<grid, block, smem, s>>>(A, off, size, sl);
+        MG_LAUNCH_CHECK();
+    };
+    switch (shape) {
+        case SH_T2: tile(lm_tile_kernel<2, WK, PREC, VER, BT>, 2); break;
+        case SH_T4: tile(lm_tile_kernel<4, WK, PREC, VER, BT>, 4); break;
+        case SH_T8: tile(lm_tile_kernel<8, WK, PREC, VER, BT>, 8); break;
+        case SH_T16: tile(lm_tile_kernel<16, WK, PREC, VER, BT>, 16); break;
+        case SH_T32: tile(lm_tile_kernel<32, WK, PREC, VER, BT>, 32); break;
+        case SH_H32: hash(lm_hash_kernel<32, WK, PREC, VER, 256, BT>, 32, 256); break;
+        case SH_H64: hash(lm_hash_kernel<64, WK, PREC, VER, 256, BT>, 64, 256); break;
+        case SH_H128: hash(lm_hash_kernel<128, WK, PREC, VER, 128, BT>, 128, 128); break;
+        case SH_H256: hash(lm_hash_kernel<256, WK, PREC, VER, 256, BT>, 256, 256); break;
+        case SH_H512: hash(lm_hash_kernel<512, WK, PREC, VER, 512, BT>, 512, 512); break;
+        default: throw Error(MG_ERR_INVALID, "unknown sweep shape");
+    }
+}
+
 template <int WK, int PREC, int VER, int BT>
 void launch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, const LMArgs &A, cudaStream_t s) {
     const Bins &B = lvl.bins;
-    // fork: heavy path on its own stream, the tile and hash bins on others
+    // fork: heavy path on its own stream, the light classes on two others
     MG_CUDA(cudaEventRecord(ws.ev_fork, s));
     for (int q = 0; q < 3; q++) MG_CUDA(cudaStreamWaitEvent(ws.streams[q], ws.ev_fork, 0));
     cudaStream_t sh = ws.streams[0], sm = ws.streams[1], st = ws.streams[2];
+    const uint32_t *hl = lvl.heavy_list;
     // heavy tiers, largest clusters first
     if (lvl.tier_off[5] > lvl.tier_off[4])
-        launch_cluster<16, WK, PREC, VER, BT>(A, ws.h_tier.get() + lvl.tier_off[4], lvl.tier_off[5] - lvl.tier_off[4], sh);
+        launch_cluster<16, WK, PREC, VER, BT>(A, hl + lvl.tier_off[4], lvl.tier_off[5] - lvl.tier_off[4], sh);
     if (lvl.tier_off[4] > lvl.tier_off[3])
-        launch_cluster<8, WK, PREC, VER, BT>(A, ws.h_tier.get() + lvl.tier_off[3], lvl.tier_off[4] - lvl.tier_off[3], sh);
+        launch_cluster<8, WK, PREC, VER, BT>(A, hl + lvl.tier_off[3], lvl.tier_off[4] - lvl.tier_off[3], sh);
     if (lvl.tier_off[3] > lvl.tier_off[2])
-        launch_cluster<4, WK, PREC, VER, BT>(A, ws.h_tier.get() + lvl.tier_off[2], lvl.tier_off[3] - lvl.tier_off[2], sh);
+        launch_cluster<4, WK, PREC, VER, BT>(A, hl + lvl.tier_off[2], lvl.tier_off[3] - lvl.tier_off[2], sh);
     if (lvl.tier_off[2] > lvl.tier_off[1])
-        launch_cluster<2, WK, PREC, VER, BT>(A, ws.h_tier.get() + lvl.tier_off[1], lvl.tier_off[2] - lvl.tier_off[1], sh);
+        launch_cluster<2, WK, PREC, VER, BT>(A, hl + lvl.tier_off[1], lvl.tier_off[2] - lvl.tier_off[1], sh);
     if (lvl.tier_off[1] > lvl.tier_off[0])
-        launch_cluster<1, WK, PREC, VER, BT>(A, ws.h_tier.get() + lvl.tier_off[0], lvl.tier_off[1] - lvl.tier_off[0], sm);
+        launch_cluster<1, WK, PREC, VER, BT>(A, hl + lvl.tier_off[0], lvl.tier_off[1] - lvl.tier_off[0], sm);
     if (lvl.giants > 0) {
         const uint32_t H = lvl.giants;
-        const uint32_t *hv = ws.h_tier.get() + lvl.tier_off[kTiers - 1];
+        const uint32_t *hv = hl + lvl.tier_off[kTiers - 1];
         heavy_insert_kernel<WK, VER, BT><<<lvl.ins_items, kHeavyThreads, 0, sh>>>(
             A, hv, H, ws.h_ins.get(), ws.h_toff.get(), ws.h_tsize.get(), ws.h_keys.get(), ws.h_vals.get(),
             ws.h_acc.get());
@@ -1097,48 +1100,32 @@ void launch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, c
                                                                                   ws.h_acc.get(), ws.h_best.get());
         MG_LAUNCH_CHECK();
     }
-    using V = typename ValT<WK>::type;
-    auto hash_launch = [&](auto kern, int slots, int gpb, int block, int bin, cudaStream_t str) {
-        if (B.size[bin] == 0) return;
-        size_t smem = (size_t)slots * gpb * (sizeof(uint32_t) + sizeof(V) + sizeof(uint16_t) / 2);
-        MG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(B.size[bin], gpb), 148ull * 64);
-        kern<<<grid, block, smem, str>>>(A, B.offset[bin], B.size[bin]);
-        MG_LAUNCH_CHECK();
-    };
-    hash_launch(lm_hash_kernel<512, 8192, WK, PREC, VER, 512, BT>, 8192, 1, 512, 8, sm);
-    hash_launch(lm_hash_kernel<256, 4096, WK, PREC, VER, 256, BT>, 4096, 1, 256, 7, sm);
-    hash_launch(lm_hash_kernel<128, 1024, WK, PREC, VER, 128, BT>, 1024, 1, 128, 6, sm);
-    hash_launch(lm_hash_kernel<32, 256, WK, PREC, VER, 256, BT>, 256, 8, 256, 5, st);
-    auto tile_launch = [&](auto kern, int T, int bin, cudaStream_t str) {
-        if (B.size[bin] == 0) return;
-        uint64_t groups_per_block = 256 / T;
-        unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(B.size[bin], groups_per_block), 148ull * 32);
-        kern<<<grid, 256, 0, str>>>(A, B.offset[bin], B.size[bin]);
-        MG_LAUNCH_CHECK();
-    };
-    tile_launch(lm_tile_kernel<32, WK, PREC, VER, BT>, 32, 4, st);
-    tile_launch(lm_tile_kernel<16, WK, PREC, VER, BT>, 16, 3, st);
-    tile_launch(lm_tile_kernel<8, WK, PREC, VER, BT>, 8, 2, st);
-    tile_launch(lm_tile_kernel<4, WK, PREC, VER, BT>, 4, 1, st);
-    tile_launch(lm_tile_kernel<2, WK, PREC, VER, BT>, 2, 0, st);
+    // light classes, heaviest first; tiles and warp tables on one stream,
+    // block tables on the other
+    for (int c = kLightClasses - 1; c >= 0; c--) {
+        const int sh_c = lvl.shape[c];
+        launch_light<WK, PREC, VER, BT>(sh_c, c, A, B.offset[c], B.size[c], sh_c <= SH_H32 ? st : sm);
+    }
     for (int q = 0; q < 3; q++) {
         MG_CUDA(cudaEventRecord(ws.ev_join[q], ws.streams[q]));
         MG_CUDA(cudaStreamWaitEvent(s, ws.ev_join[q], 0));
     }
 }
 
-// Weight kind / precision / version dispatch of one sweep.
-template <int BT>
-void dispatch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p,
-                    const LMArgs &A, cudaStream_t s) {
+// The kernel weight kind a sweep of g uses (integral graphs: integer slots).
+inline int sweep_wk(const GraphView &g, const SweepParams &p) {
+    return p.integral ? (g.wk == WK_F32 ? (int)WK_F32I : g.wk == WK_F64 ? (int)WK_F64I : g.wk) : g.wk;
+}
+
+// Weight kind / precision / version dispatch: f.run<WK, PREC, VER>().
+template <class F>
+void dispatch_kind(const GraphView &g, const SweepParams &p, F &f) {
     MG_CHECK(p.version == 1 || p.version == 2, MG_ERR_INVALID, "version must be 0, 1 or 2");
-    // integral graphs accumulate in integer table slots
-    const int wk = p.integral ? (g.wk == WK_F32 ? (int)WK_F32I : g.wk == WK_F64 ? (int)WK_F64I : g.wk) : g.wk;
+    const int wk = sweep_wk(g, p);
 #define MG_SWEEP_CASE(WKV, PRECV)                                                                  \
     if (wk == WKV && p.precision == PRECV) {                                                       \
-        if (p.version == 1) launch_sweep<WKV, PRECV, 1, BT>(g, lvl, ws, A, s);                     \
-        else launch_sweep<WKV, PRECV, 2, BT>(g, lvl, ws, A, s);                                    \
+        if (p.version == 1) f.template run<WKV, PRECV, 1>();                                       \
+        else f.template run<WKV, PRECV, 2>();                                                      \
         return;                                                                                    \
     }
     MG_SWEEP_CASE(WK_UNIT, MG_PREC_FP64)
@@ -1156,6 +1143,114 @@ void dispatch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws,
     MG_SWEEP_CASE(WK_F64, MG_PREC_FP32)
 #undef MG_SWEEP_CASE
     throw Error(MG_ERR_INVALID, "unknown weight kind or precision");
+}
+
+template <int BT>
+struct SweepF {
+    const GraphView &g;
+    const MoveLevel &lvl;
+    MoveWorkspace &ws;
+    const LMArgs &A;
+    cudaStream_t s;
+    template <int WK, int PREC, int VER>
+    void run() {
+        launch_sweep<WK, PREC, VER, BT>(g, lvl, ws, A, s);
+    }
+};
+
+template <int BT>
+struct LightF {
+    int shape, cls;
+    const LMArgs &A;
+    uint32_t off, size;
+    cudaStream_t s;
+    template <int WK, int PREC, int VER>
+    void run() {
+        launch_light<WK, PREC, VER, BT>(shape, cls, A, off, size, s);
+    }
+};
+
+// A full sweep.
+template <int BT>
+void dispatch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p,
+                    const LMArgs &A, cudaStream_t s) {
+    SweepF<BT> f{g, lvl, ws, A, s};
+    dispatch_kind(g, p, f);
+}
+
+// One light class alone on stream s (the autotuner's timing runs).
+template <int BT>
+void dispatch_light(const GraphView &g, const SweepParams &p, const LMArgs &A, int shape, int cls, uint32_t off,
+                    uint32_t size, cudaStream_t s) {
+    LightF<BT> f{shape, cls, A, off, size, s};
+    dispatch_kind(g, p, f);
+}
+
+// Candidate shapes of light class cls (degrees <= 2^cls): shapes whose table
+// holds the class, from the thinnest that fits to a few wider ones.
+inline std::vector<int> tune_candidates(int cls) {
+    const uint32_t maxdeg = 1u << cls;
+    std::vector<int> out;
+    if (cls <= 5) {
+        const int t0 = cls <= 1 ? SH_T2 : SH_T2 + (cls - 1);
+        out.push_back(t0);
+        if (t0 < SH_T32) out.push_back(t0 + 1);
+        out.push_back(SH_H32);
+        return out;
+    }
+    for (int sh = SH_H32; sh <= SH_H512; sh++) {
+        if (shape_capacity(sh) < maxdeg) continue;
+        // wider groups than twice the degree leave most threads idle
+        const uint32_t gt = 32u << (sh - SH_H32);
+        if (gt > 2 * maxdeg && sh > SH_H32) continue;
+        out.push_back(sh);
+        if (out.size() == 3) break;
+    }
+    return out;
+}
+
+// Fill lvl.shape from the table; time the candidates of classes missing from
+// it (MG_TUNE_ON).  A timing run is a normal launch of that class: it writes
+// the same new assignment the sweep will write; its sums go to ws.tune_acc.
+template <int BT>
+void tune_light(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p, LMArgs A,
+                cudaStream_t s) {
+    for (int c = 0; c < kLightClasses; c++) lvl.shape[c] = (uint8_t)default_shape(c);
+    TuneTable &T = ws.tune;
+    if (T.mode == MG_TUNE_OFF) return;
+    A.acc = ws.tune_acc.ensure(1);
+    const int wk = sweep_wk(g, p);
+    cudaEvent_t e0 = ws.ev_tune[0], e1 = ws.ev_tune[1];
+    for (int c = 0; c < kLightClasses; c++) {
+        const uint32_t size = lvl.bins.size[c];
+        if (size < kTuneMinVertices) continue;
+        const uint32_t key = TuneTable::key(wk, p.precision, p.version, BT, c, size);
+        auto it = T.entries.find(key);
+        if (it != T.entries.end()) {
+            lvl.shape[c] = it->second.shape;
+            continue;
+        }
+        if (T.mode != MG_TUNE_ON) continue;
+        float best = 1e30f;
+        int best_sh = default_shape(c);
+        for (int sh : tune_candidates(c)) {
+            float ms = 0;
+            for (int rep = 0; rep < 2; rep++) {  // the first run also loads the kernel
+                MG_CUDA(cudaEventRecord(e0, s));
+                dispatch_light<BT>(g, p, A, sh, c, lvl.bins.offset[c], size, s);
+                MG_CUDA(cudaEventRecord(e1, s));
+                MG_CUDA(cudaEventSynchronize(e1));
+                MG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            }
+            if (ms < best) {
+                best = ms;
+                best_sh = sh;
+            }
+        }
+        T.entries[key] = TuneEntry{(uint8_t)best_sh, best * 1000.0f};
+        T.tuned++;
+        lvl.shape[c] = (uint8_t)best_sh;
+    }
 }
 
 }  // namespace lmk

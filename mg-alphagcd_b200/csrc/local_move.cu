@@ -36,11 +36,6 @@ namespace {
 
 using namespace lmk;
 
-__global__ void heavy_degree_kernel(const uint32_t *off, const uint32_t *hv, uint32_t H, uint32_t *deg) {
-    uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
-    if (h < H) deg[h] = off[hv[h] + 1] - off[hv[h]];
-}
-
 __global__ void heavy_layout_kernel(const uint32_t *off, const uint32_t *hv, uint32_t H, uint32_t *tsize,
                                     uint32_t *ins_cnt, uint32_t *eval_cnt, uint64_t *tsz64) {
     uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
@@ -128,11 +123,26 @@ int probe_max_cluster() {
 
 }  // namespace
 
+const char *shape_name(int sh) {
+    static const char *names[SH_COUNT] = {"t2", "t4", "t8", "t16", "t32", "h32", "h64", "h128", "h256", "h512"};
+    return sh >= 0 && sh < SH_COUNT ? names[sh] : "?";
+}
+
+// The shapes before any tuning: T-lane tiles up to degree 32, a warp per
+// vertex up to 128, then 128 / 256 / 512 threads per vertex.
+int default_shape(int cls) {
+    static const uint8_t d[kLightClasses] = {SH_T2,  SH_T2,   SH_T4,   SH_T8,   SH_T16,  SH_T32, SH_H32,
+                                             SH_H32, SH_H128, SH_H128, SH_H256, SH_H256, SH_H512};
+    return cls >= 0 && cls < kLightClasses ? d[cls] : SH_H512;
+}
+
 MoveWorkspace::~MoveWorkspace() {
     for (auto &s : streams)
         if (s) cudaStreamDestroy(s);
     if (ev_fork) cudaEventDestroy(ev_fork);
     for (auto &e : ev_join)
+        if (e) cudaEventDestroy(e);
+    for (auto &e : ev_tune)
         if (e) cudaEventDestroy(e);
 }
 
@@ -141,57 +151,34 @@ void MoveWorkspace::init_streams() {
     for (auto &s : streams) MG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     MG_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
     for (auto &e : ev_join) MG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (auto &e : ev_tune) MG_CUDA(cudaEventCreate(&e));
 }
 
 void move_prepare_level(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, cudaStream_t s) {
     ws.init_streams();
     ws.acc.ensure(1);
     uint32_t *perm = ws.perm.ensure(g.n + 1);
-    compute_bins(0, g.n, g.off, perm, lvl.bins, s, ws.prim);
-    lvl.heavy = lvl.bins.size[9];
+    compute_bins(kSweepScheme, g.n, g.off, perm, lvl.bins, s, ws.prim);
+    for (int c = 0; c < kLightClasses; c++) lvl.shape[c] = (uint8_t)default_shape(c);
+    const uint32_t h0 = lvl.bins.offset[kFirstHeavyClass];
+    lvl.heavy = g.n - h0;
+    lvl.heavy_list = perm + h0;
     lvl.ins_items = lvl.eval_items = 0;
     lvl.table_slots = 0;
     lvl.giants = 0;
     for (int t = 0; t <= kTiers; t++) lvl.tier_off[t] = 0;
     if (lvl.heavy == 0) return;
     if (ws.max_cluster == 0) ws.max_cluster = probe_max_cluster();
-    // tiers by degree: tier t (cluster of 2^t CTAs) takes deg <= 2^t * S / 2
-    {
-        const uint32_t Hall = lvl.heavy;
-        const uint32_t *hall = perm + lvl.bins.offset[9];
-        uint32_t *deg = ws.h_deg.ensure(Hall + 1);
-        heavy_degree_kernel<<<(unsigned)ceil_div(Hall, 256), 256, 0, s>>>(g.off, hall, Hall, deg);
-        MG_LAUNCH_CHECK();
-        std::vector<uint32_t> hv_h(Hall), dg_h(Hall);
-        MG_CUDA(cudaMemcpyAsync(hv_h.data(), hall, sizeof(uint32_t) * Hall, cudaMemcpyDeviceToHost, s));
-        MG_CUDA(cudaMemcpyAsync(dg_h.data(), deg, sizeof(uint32_t) * Hall, cudaMemcpyDeviceToHost, s));
-        MG_CUDA(cudaStreamSynchronize(s));
-        std::vector<uint32_t> lists[kTiers];
-        const int top = ws.max_cluster >= 16 ? 4 : 3;
-        for (uint32_t h = 0; h < Hall; h++) {
-            int t = kTiers - 1;
-            for (int c = 0; c <= top; c++)
-                if ((uint64_t)dg_h[h] <= (uint64_t)(kClusterSlots / 2) << c) {
-                    t = c;
-                    break;
-                }
-            lists[t].push_back(hv_h[h]);
-        }
-        std::vector<uint32_t> tiered;
-        tiered.reserve(Hall);
-        for (int t = 0; t < kTiers; t++) {
-            lvl.tier_off[t] = (uint32_t)tiered.size();
-            tiered.insert(tiered.end(), lists[t].begin(), lists[t].end());
-        }
-        lvl.tier_off[kTiers] = (uint32_t)tiered.size();
-        MG_CUDA(cudaMemcpyAsync(ws.h_tier.ensure(Hall + 1), tiered.data(), sizeof(uint32_t) * Hall,
-                                cudaMemcpyHostToDevice, s));
-        lvl.giants = lvl.tier_off[kTiers] - lvl.tier_off[kTiers - 1];
-        MG_CUDA(cudaStreamSynchronize(s));
-    }
+    // classes 13..17 are the cluster tiers of 1..16 CTAs (a tier of 2^t CTAs
+    // holds degrees up to 2^t * kClusterSlots / 2), class 18 the giants; on a
+    // device without 16-CTA clusters class 17 joins the giants
+    for (int t = 0; t < kTiers; t++) lvl.tier_off[t] = lvl.bins.offset[kFirstHeavyClass + t] - h0;
+    lvl.tier_off[kTiers] = lvl.heavy;
+    if (ws.max_cluster < 16) lvl.tier_off[kTiers - 1] = lvl.tier_off[kTiers - 2];
+    lvl.giants = lvl.tier_off[kTiers] - lvl.tier_off[kTiers - 1];
     if (lvl.giants == 0) return;
     const uint32_t H = lvl.giants;
-    const uint32_t *hv = ws.h_tier.get() + lvl.tier_off[kTiers - 1];
+    const uint32_t *hv = lvl.heavy_list + lvl.tier_off[kTiers - 1];
     uint32_t *tsize = ws.h_tsize.ensure(H + 1);
     uint32_t *ins = ws.h_ins.ensure(H + 1);
     uint32_t *ev = ws.h_eval.ensure(H + 1);
@@ -238,8 +225,9 @@ GainK gain_constants(double mass) {
     return K;
 }
 
-void move_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p,
-                const uint32_t *P, uint32_t *N, const double *k, const double *sigma, cudaStream_t s) {
+namespace {
+LMArgs single_args(const GraphView &g, MoveWorkspace &ws, const SweepParams &p, const uint32_t *P, uint32_t *N,
+                   const double *k, const double *sigma) {
     LMArgs A = {};
     A.off = g.off;
     A.col = g.col;
@@ -256,7 +244,19 @@ void move_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, con
     if (p.precision == MG_PREC_INT64)
         MG_CHECK(p.integral && p.mass < 2147483648.0, MG_ERR_UNSUPPORTED,
                  "int64 precision needs integral weights with total below 2^31");
+    return A;
+}
+}  // namespace
+
+void move_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p,
+                const uint32_t *P, uint32_t *N, const double *k, const double *sigma, cudaStream_t s) {
+    const LMArgs A = single_args(g, ws, p, P, N, k, sigma);
     dispatch_sweep<0>(g, lvl, ws, p, A, s);
+}
+
+void move_tune(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p, const uint32_t *P,
+               uint32_t *N, const double *k, const double *sigma, cudaStream_t s) {
+    tune_light<0>(g, lvl, ws, p, single_args(g, ws, p, P, N, k, sigma), s);
 }
 
 void sigma_sumsq(const double *sigma, uint32_t n, int integral, MoveWorkspace &ws, cudaStream_t s) {

@@ -11,8 +11,9 @@ namespace mg {
 
 using namespace lmk;
 
-void move_sweep_batch(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p,
-                      const BatchSweep &b, const double *k, const double *sigma, cudaStream_t s) {
+namespace {
+LMArgs batch_args(const GraphView &g, MoveWorkspace &ws, const SweepParams &p, const BatchSweep &b, const double *k,
+                  const double *sigma) {
     LMArgs A = {};
     A.off = g.off;
     A.col = g.col;
@@ -31,7 +32,19 @@ void move_sweep_batch(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &w
     A.Cb2 = b.C[2];
     A.sinv = b.sinv;
     A.up_dev = b.up;
+    return A;
+}
+}  // namespace
+
+void move_sweep_batch(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p,
+                      const BatchSweep &b, const double *k, const double *sigma, cudaStream_t s) {
+    const LMArgs A = batch_args(g, ws, p, b, k, sigma);
     dispatch_sweep<1>(g, lvl, ws, p, A, s);
+}
+
+void move_tune_batch(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p,
+                     const BatchSweep &b, const double *k, const double *sigma, cudaStream_t s) {
+    tune_light<1>(g, lvl, ws, p, batch_args(g, ws, p, b, k, sigma), s);
 }
 
 }  // namespace mg

@@ -113,6 +113,9 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
         int base = 0, pend = 1;
         // first sweep: P = identity (base), proposes C[1]; yields Q0
         sp.up = 1;
+        // shapes of the light classes (autotuner; its timing runs write the
+        // proposal this sweep writes)
+        move_tune(cur, mlv, ctx->mws, sp, C[base], C[pend], k, sigma, s);
         sweep_reset_acc(ctx->mws, s);
         sigma_sumsq(sigma, n, integral, ctx->mws, s);
         MG_CUDA(cudaEventRecord(ctx->ev[4], s));
