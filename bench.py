@@ -16,6 +16,14 @@ unit weights) -- graphs/s of one batched run against the graphs/s of a loop
 of single-graph runs over a systematic sample of the same graphs, and a check
 that every sampled graph got the same modularity both ways.
 
+Two more single-graph workloads are reported beside it: "sbm64k" (seeded SBM,
+65,536 vertices in 64 planted communities, mean degree 16, 80% intra: Q and
+the community count of every level) and "precision" (seeded Chung-Lu graph,
+4,194,304 vertices, exponent 2.1, mean degree 20, degrees capped at 200,000,
+float lognormal(0, 1) weights: FP32 gains against FP64 gains, the FP64
+modularity recomputed from the FP32 run's assignment, and exact int64 gains
+against FP64 gains on the unit-weight copy of the same graph).
+
 It also carries "serving": a Poisson stream of Louvain jobs (default 200
 requests/s for 60 s; half SBM, half R-MAT with edge factor 16 and the
 R-MAT-24 probabilities; vertex counts log-uniform in [1k, 8M]) submitted to
@@ -62,6 +70,7 @@ def parse():
     ap.add_argument("--batch-graphs", type=int, default=4096)
     ap.add_argument("--batch-steps", type=int, default=2)
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the sbm64k and precision lines")
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     return ap.parse_args()
@@ -226,6 +235,50 @@ def run_reference(args, world, rank, local, pg):
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     return line
+
+
+def _timed_runs(g, k, **kw):
+    g.louvain(**kw)  # warm-up (and autotuning of new degree classes)
+    runs = [g.louvain(**kw) for _ in range(k)]
+    return runs, statistics.median(r["seconds_total"] for r in runs)
+
+
+def run_sbm64k(ctx):
+    g = ctx.generate_sbm(65536, 64, 16.0, 0.8, 1)
+    info = g.info()
+    runs, t = _timed_runs(g, 3)
+    r = runs[-1]
+    g.close()
+    return {"workload": "SBM 65,536 vertices, 64 blocks, mean degree 16, 80% intra, seed 1, unit weights",
+            "directed_entries": info["nnz"], "modularity": r["modularity"], "communities": r["communities"],
+            "vertices_per_level": [int(x) for x in r["level_sizes"]], "phases": r["phases"],
+            "iterations": r["iterations"], "run_s": t, "edges_per_s": r["edges_swept"] / r["seconds_total"]}
+
+
+def run_precision(ctx):
+    n = 4_194_304
+    gw = ctx.generate_chunglu(n, 2.1, 20.0, 200000.0, lognormal=True, seed=3)
+    info = gw.info()
+    r64, t64 = _timed_runs(gw, 2, precision="fp64")
+    r32, t32 = _timed_runs(gw, 2, precision="fp32")
+    q64, q32 = r64[-1]["modularity"], r32[-1]["modularity"]
+    q32_fp64 = gw.modularity(r32[-1]["assignment"])
+    gw.close()
+    gu = ctx.generate_chunglu(n, 2.1, 20.0, 200000.0, lognormal=False, seed=3)
+    u64, tu64 = _timed_runs(gu, 2, precision="fp64")
+    ui, tui = _timed_runs(gu, 2, precision="int64")
+    gu.close()
+    return {"workload": "Chung-Lu 4,194,304 vertices, exponent 2.1, mean degree 20, max degree 200,000, seed 3",
+            "directed_entries": info["nnz"],
+            "lognormal_f32_weights": {"fp64": {"modularity": q64, "run_s": t64},
+                                      "fp32": {"modularity": q32, "run_s": t32,
+                                               "modularity_recomputed_fp64": q32_fp64},
+                                      "fp32_vs_fp64_abs_error": abs(q32 - q64),
+                                      "fp32_reported_vs_recomputed_abs_error": abs(q32 - q32_fp64)},
+            "unit_weights": {"fp64": {"modularity": u64[-1]["modularity"], "run_s": tu64},
+                             "int64": {"modularity": ui[-1]["modularity"], "run_s": tui},
+                             "int64_vs_fp64_abs_error": abs(ui[-1]["modularity"] - u64[-1]["modularity"]),
+                             "same_assignment": bool((ui[-1]["assignment"] == u64[-1]["assignment"]).all())}}
 
 
 BATCH = dict(n_range=(1000, 200000), blocks_range=(4, 256), deg_range=(8.0, 32.0), intra_range=(0.7, 0.9), seed=4)
@@ -400,7 +453,11 @@ def run_engine(args, world, rank, local, pg):
                "sample": f"one phase-0 sweep (local move + sigma update + modularity) over the same graph, "
                          f"{ct_:.1f} s on {threads} threads"}
         del csr
-    batched = serving = None
+    batched = serving = sbm64k = precision = None
+    if world == 1 and not args.no_extra:
+        g.close()
+        sbm64k = run_sbm64k(ctx)
+        precision = run_precision(ctx)
     if world == 1 and not args.no_batched:
         g.close()
         batched = run_batched(mg, ctx, args)
@@ -434,6 +491,8 @@ def run_engine(args, world, rank, local, pg):
                 "d2h_bytes_per_step": 4 * info["n"]},
         "clocks": clk,
         "gpu_launches": int(sum(r["kernel_launches"] for r in runs)),
+        "sbm64k": sbm64k,
+        "precision": precision,
         "batched": batched,
         "serving": serving,
     }

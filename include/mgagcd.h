@@ -91,6 +91,14 @@ mg_status mg_graph_generate_rmat(mg_ctx *ctx, int scale, int edge_factor, double
                                  uint64_t seed, mg_graph **out);
 mg_status mg_graph_generate_sbm(mg_ctx *ctx, uint32_t n, uint32_t blocks, double mean_degree,
                                 double intra_frac, uint64_t seed, mg_graph **out);
+/* Chung-Lu power-law graph: expected degree of vertex i proportional to
+ * (i + i0)^(-1/(exponent-1)), mean mean_degree, capped at max_degree;
+ * lognormal = 1 gives every edge a weight lognormal(0, 1) rounded to float
+ * (stored as f32), else unit weights.  The same seed gives the same topology
+ * with and without weights, and the same topology as the test oracle's
+ * generator. */
+mg_status mg_graph_generate_chunglu(mg_ctx *ctx, uint32_t n, double exponent, double mean_degree,
+                                    double max_degree, int lognormal, uint64_t seed, mg_graph **out);
 
 /* n, nnz, mass (sum of all directed weights, src/graph/host_graph.cpp:112-115),
  * integral (1 when every weight is a non-negative integer and mass < 2^32). */

@@ -114,7 +114,7 @@ EXPORTED = [
     "mg_batch_result_assignment", "mg_batch_result_destroy", "mg_batch_generate", "mg_serve_start",
     "mg_serve_submit", "mg_serve_submit_csr", "mg_serve_poll", "mg_serve_wait", "mg_serve_assignment",
     "mg_serve_cancel", "mg_serve_release", "mg_serve_stats", "mg_serve_last_error", "mg_serve_stop",
-    "mg_tune_mode", "mg_tune_table", "mg_tune_save", "mg_tune_load",
+    "mg_tune_mode", "mg_tune_table", "mg_tune_save", "mg_tune_load", "mg_graph_generate_chunglu",
 ]
 TUNE_OFF, TUNE_CACHED, TUNE_ON = 0, 1, 2
 
@@ -142,6 +142,7 @@ def lib():
     L.mg_graph_from_mtx.argtypes = [vp, ct.c_char_p, pp]
     L.mg_graph_generate_rmat.argtypes = [vp, i32, i32, dbl, dbl, dbl, u64, pp]
     L.mg_graph_generate_sbm.argtypes = [vp, u32, u32, dbl, dbl, u64, pp]
+    L.mg_graph_generate_chunglu.argtypes = [vp, u32, dbl, dbl, dbl, i32, u64, pp]
     L.mg_graph_info.argtypes = [vp, ct.POINTER(u32), ct.POINTER(u64), ct.POINTER(dbl), ct.POINTER(i32)]
     L.mg_graph_copy_csr.argtypes = [vp, vp, vp, vp]
     L.mg_graph_destroy.argtypes = [vp]
@@ -254,6 +255,13 @@ class Context:
         h = ct.c_void_p()
         self.check(lib().mg_graph_generate_sbm(self.h, n, blocks, mean_degree, intra_frac, seed, ct.byref(h)),
                    "mg_graph_generate_sbm")
+        return Graph(self, h)
+
+    def generate_chunglu(self, n: int, exponent: float = 2.1, mean_degree: float = 20.0,
+                         max_degree: float = 200000.0, lognormal: bool = True, seed: int = 3) -> "Graph":
+        h = ct.c_void_p()
+        self.check(lib().mg_graph_generate_chunglu(self.h, n, exponent, mean_degree, max_degree, int(lognormal), seed,
+                                                   ct.byref(h)), "mg_graph_generate_chunglu")
         return Graph(self, h)
 
     def bins_offsets(self, scheme: int, offsets) -> dict:

@@ -211,6 +211,22 @@ mg_status mg_graph_generate_sbm(mg_ctx *ctx, uint32_t n, uint32_t blocks, double
     return MG_OK;
 }
 
+mg_status mg_graph_generate_chunglu(mg_ctx *ctx, uint32_t n, double exponent, double mean_degree, double max_degree,
+                                    int lognormal, uint64_t seed, mg_graph **out) {
+    if (!ctx || !out) return fail(ctx, MG_ERR_INVALID, "mg_graph_generate_chunglu: NULL argument");
+    *out = nullptr;
+    mg_graph *g = new (std::nothrow) mg_graph();
+    if (!g) return fail(ctx, MG_ERR_OOM, "host allocation failed");
+    g->ctx = ctx;
+    mg_status st = guarded(ctx, [&] { graph_generate_chunglu(g, n, exponent, mean_degree, max_degree, lognormal, seed); });
+    if (st != MG_OK) {
+        delete g;
+        return st;
+    }
+    *out = g;
+    return MG_OK;
+}
+
 mg_status mg_graph_info(const mg_graph *g, uint32_t *n, uint64_t *nnz, double *mass, int *integral) {
     if (!g) return MG_ERR_INVALID;
     if (n) *n = g->n;

@@ -168,6 +168,20 @@ __global__ void pair_keys_kernel(const uint32_t *u, const uint32_t *v, uint64_t 
     }
 }
 
+// weighted pairs: both directions carry the pair's weight
+__global__ void pair_weights_kernel(const double *w, uint64_t m, double *vals) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+        vals[2 * i] = w[i];
+        vals[2 * i + 1] = w[i];
+    }
+}
+
+// weight of each unique key: the first of its run (duplicate pairs of a
+// generator carry equal weights)
+__global__ void run_first_values_kernel(const uint32_t *ustart, uint32_t u, const double *vals, double *w) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < u; s += gridDim.x * blockDim.x) w[s] = vals[ustart[s]];
+}
+
 __global__ void gather_compose_kernel(uint32_t *assign, const uint32_t *map, uint32_t n0) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n0; v += gridDim.x * blockDim.x)
         assign[v] = map[assign[v]];
@@ -295,7 +309,7 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
 }
 
 void csr_from_device_pairs(uint32_t n, uint64_t m, const uint32_t *u, const uint32_t *v, LevelGraph &out,
-                           CoarsenWorkspace &ws, cudaStream_t s) {
+                           CoarsenWorkspace &ws, cudaStream_t s, const double *w) {
     const size_t mm = 2 * m;
     MG_CHECK(mm < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "graph has more than 2^32-1 directed entries");
     if (m == 0) {
@@ -303,6 +317,7 @@ void csr_from_device_pairs(uint32_t n, uint64_t m, const uint32_t *u, const uint
         out.nnz = 0;
         MG_CUDA(cudaMemsetAsync(out.off.ensure((size_t)n + 1), 0, sizeof(uint32_t) * ((size_t)n + 1), s));
         out.col.ensure(1);
+        out.w.ensure(1);
         return;
     }
     const int bc = bits_for(n);
@@ -311,7 +326,17 @@ void csr_from_device_pairs(uint32_t n, uint64_t m, const uint32_t *u, const uint
     pair_keys_kernel<<<grid_for(m), 256, 0, s>>>(u, v, m, bc, keys);
     MG_LAUNCH_CHECK();
     // self-loop markers (bit 2*bc set) sort last and are dropped below
-    bool flipped = radix_sort<NoVal>(keys, (NoVal *)nullptr, keys2, (NoVal *)nullptr, mm, 2 * bc + 1, s, ws.prim);
+    bool flipped;
+    const double *sv = nullptr;
+    if (w) {
+        double *vals = ws.vals.ensure(mm + 1), *vals2 = ws.vals_alt.ensure(mm + 1);
+        pair_weights_kernel<<<grid_for(m), 256, 0, s>>>(w, m, vals);
+        MG_LAUNCH_CHECK();
+        flipped = radix_sort<double>(keys, vals, keys2, vals2, mm, 2 * bc + 1, s, ws.prim);
+        sv = flipped ? vals2 : vals;
+    } else {
+        flipped = radix_sort<NoVal>(keys, (NoVal *)nullptr, keys2, (NoVal *)nullptr, mm, 2 * bc + 1, s, ws.prim);
+    }
     const uint64_t *sk = flipped ? keys2 : keys;
     uint32_t *head = ws.rowcnt.ensure(mm + 1);
     uint32_t *seg = ws.seg.ensure(mm + 1);
@@ -336,6 +361,10 @@ void csr_from_device_pairs(uint32_t n, uint64_t m, const uint32_t *u, const uint
         MG_CUDA(cudaMemsetAsync(off, 0, sizeof(uint32_t) * ((size_t)n + 1), s));
     } else {
         emit_rows(ukey, uu, bc, n, off, col, s);
+        if (w) {
+            run_first_values_kernel<<<grid_for(uu), 256, 0, s>>>(ustart, uu, sv, out.w.ensure((size_t)uu + 1));
+            MG_LAUNCH_CHECK();
+        }
     }
 }
 

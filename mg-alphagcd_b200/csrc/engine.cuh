@@ -253,9 +253,10 @@ void coarsen_level(const GraphView &g, const uint32_t *C_dense, uint32_t n_new, 
                    CoarsenWorkspace &ws, cudaStream_t s, uint64_t *upper_degree_off /* device, may be null */);
 
 // Build a symmetric deduplicated CSR from undirected pairs already on the
-// device (self-loops dropped); used by the generators.
+// device (self-loops dropped); used by the generators.  With pair weights w
+// (equal for duplicate pairs), out.w receives the weight of every entry.
 void csr_from_device_pairs(uint32_t n, uint64_t m, const uint32_t *u, const uint32_t *v, LevelGraph &out,
-                           CoarsenWorkspace &ws, cudaStream_t s);
+                           CoarsenWorkspace &ws, cudaStream_t s, const double *w = nullptr);
 
 // device-side helpers
 void gather_compose(uint32_t *assign, const uint32_t *map, uint32_t n0, cudaStream_t s);

@@ -71,6 +71,43 @@ __global__ void sbm_pairs_kernel(uint32_t n, uint32_t blocks, uint64_t min_, uin
         sbm_pair(n, blocks, min_, kin, kout, k, u[k], v[k]);
 }
 
+// Chung-Lu pair k: both endpoints drawn from the expected-degree distribution
+// (first index whose 63-bit cumulative weight exceeds a 63-bit random draw);
+// the pair's weight, when asked for, is lognormal(0, 1) rounded to float, a
+// function of the unordered pair (Box-Muller on two hashes of it)
+__global__ void chunglu_pairs_kernel(const uint64_t *cdf, uint32_t n, uint64_t m, uint64_t key, uint64_t kw,
+                                     uint32_t *u, uint32_t *v, double *w) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t ends[2];
+        for (int side = 0; side < 2; side++) {
+            const uint64_t x = rng_at(key, 2 * k + side) >> 1;
+            uint32_t a = 0, b = n - 1;
+            while (a < b) {
+                const uint32_t mid = a + (b - a) / 2;
+                if (cdf[mid] > x) b = mid;
+                else a = mid + 1;
+            }
+            ends[side] = a;
+        }
+        u[k] = ends[0];
+        v[k] = ends[1];
+        if (w) {
+            const uint32_t a = min(ends[0], ends[1]), b = max(ends[0], ends[1]);
+            const uint64_t h1 = mix64(kw ^ (((uint64_t)a << 32) | b));
+            const uint64_t h2 = mix64(h1);
+            const double u1 = ((double)(h1 >> 11) + 1.0) * (1.0 / 9007199254740992.0);
+            const double u2 = (double)(h2 >> 11) * (1.0 / 9007199254740992.0);
+            const double z = sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+            w[k] = (double)(float)exp(z);
+        }
+    }
+}
+
+__global__ void to_f32_kernel(const double *x, uint64_t m, float *y) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x)
+        y[i] = (float)x[i];
+}
+
 // per-graph parameters of a generated batch
 struct GenDev {
     uint32_t kind, n, blocks, vbase;  // SBM: vertices, blocks; first vertex in the union
@@ -361,6 +398,93 @@ void graph_generate_sbm(mg_graph *g, uint32_t n, uint32_t blocks, double mean_de
         MG_LAUNCH_CHECK();
     }
     finish_generated(g, n, m, u, v);
+}
+
+// Seeded Chung-Lu graph: expected degrees w_i = c * (i + i0)^(-1/(exponent-1)),
+// i0 chosen so that w_0 / mean(w) = max_degree / mean_degree (integral
+// approximation, bisection), scaled to mean_degree and capped at max_degree;
+// n * mean_degree / 2 pairs with both ends drawn with probability
+// proportional to w; self-loops dropped, duplicates merged.  The expected
+// degrees and their cumulative table are computed on the host in the order
+// written (the same table as the test oracle's generator); the pairs on the
+// device from the same counter-based stream.
+void graph_generate_chunglu(mg_graph *g, uint32_t n, double exponent, double mean_degree, double max_degree,
+                            int lognormal, uint64_t seed) {
+    MG_CHECK(n >= 2 && n < 0xFFFFFFFFu && exponent > 1.0 && mean_degree > 0 && max_degree > 0, MG_ERR_INVALID,
+             "chung-lu: need n >= 2, exponent > 1, positive degrees");
+    const double alpha = 1.0 / (exponent - 1.0);
+    double lo = 1e-6, hi = (double)n;
+    for (int it = 0; it < 200; it++) {
+        const double i0 = 0.5 * (lo + hi);
+        const double integ = (alpha == 1.0) ? std::log((n + i0) / i0)
+                                            : (std::pow(n + i0, 1.0 - alpha) - std::pow(i0, 1.0 - alpha)) / (1.0 - alpha);
+        const double ratio = std::pow(i0, -alpha) / (integ / n);
+        if (ratio > max_degree / mean_degree) lo = i0;
+        else hi = i0;
+    }
+    const double i0 = 0.5 * (lo + hi);
+    std::vector<double> wd(n);
+    double sum = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        wd[i] = std::pow((double)i + i0, -alpha);
+        sum += wd[i];
+    }
+    const double cst = mean_degree * n / sum;
+    double tot = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        wd[i] *= cst;
+        if (wd[i] > max_degree) wd[i] = max_degree;
+        tot += wd[i];
+    }
+    std::vector<uint64_t> cdf(n);
+    double acc = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        acc += wd[i];
+        double f = acc / tot;
+        if (f > 1.0) f = 1.0;
+        cdf[i] = (uint64_t)(f * 9223372036854775808.0);
+    }
+    cdf[n - 1] = 0x8000000000000000ull;
+    const uint64_t m = (uint64_t)std::llround((double)n * mean_degree / 2.0);
+    MG_CHECK(2 * m < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "chung-lu: more than 2^32-1 directed entries");
+    mg_ctx *ctx = g->ctx;
+    cudaStream_t s = ctx->stream;
+    DBuf<uint64_t> dcdf;
+    DBuf<uint32_t> u, v;
+    DBuf<double> w;
+    MG_CUDA(cudaMemcpyAsync(dcdf.ensure(n), cdf.data(), sizeof(uint64_t) * n, cudaMemcpyHostToDevice, s));
+    u.ensure(m + 1);
+    v.ensure(m + 1);
+    double *dw = lognormal ? w.ensure(m + 1) : nullptr;
+    if (m > 0) {
+        chunglu_pairs_kernel<<<148 * 16, 256, 0, s>>>(dcdf.get(), n, m, rng_key(seed, 0x434c5547ull),
+                                                      rng_key(seed, 0x4c4f474eull), u.get(), v.get(), dw);
+        MG_LAUNCH_CHECK();
+    }
+    LevelGraph lv;
+    csr_from_device_pairs(n, m, u.get(), v.get(), lv, ctx->cws, s, dw);
+    g->n = n;
+    g->nnz = lv.nnz;
+    std::swap(g->off.p, lv.off.p);
+    std::swap(g->off.cap, lv.off.cap);
+    std::swap(g->col.p, lv.col.p);
+    std::swap(g->col.cap, lv.col.cap);
+    if (!lognormal) {
+        g->wk = WK_UNIT;
+        g->mass = (double)lv.nnz;
+        g->integral = lv.nnz < 4294967296ull;
+    } else {
+        // every weight is a float value: keep them as f32
+        if (lv.nnz) {
+            to_f32_kernel<<<148 * 16, 256, 0, s>>>(lv.w.get(), lv.nnz, g->w32.ensure(lv.nnz + 1));
+            MG_LAUNCH_CHECK();
+        }
+        g->wk = WK_F32;
+        int integral = 0, unit = 0;
+        device_weight_stats<float>(g->w32.get(), lv.nnz, g->mass, integral, unit, s);
+        g->integral = integral;
+    }
+    MG_CUDA(cudaStreamSynchronize(s));
 }
 
 // ---- batches -----------------------------------------------------------------

@@ -75,7 +75,7 @@ struct BatchCtrl {
 // Device state of a batch, resident between runs.
 struct BatchWork {
     DBuf<uint32_t> gid, goff, goff_new, goff0, gword, gnnz, loops, Cf;
-    // active lists: bins 0-8 entries (perm order) and vertices (id order), each
+    // active lists: light-class entries (class order) and vertices (id order), each
     // with the graph of every entry; double-buffered for compaction
     DBuf<uint32_t> lperm[2], lpgid[2], lvert[2], lvgid[2], flags, pos;
     DBuf<double> sinv, curQ, gmass;
@@ -129,6 +129,8 @@ void graph_from_level(mg_graph *g, LevelGraph &lv, int integral, double mass);
 void graph_generate_rmat(mg_graph *g, int scale, int edge_factor, double a, double b, double c, uint64_t seed);
 void graph_generate_sbm(mg_graph *g, uint32_t n, uint32_t blocks, double mean_degree, double intra_frac,
                         uint64_t seed);
+void graph_generate_chunglu(mg_graph *g, uint32_t n, double exponent, double mean_degree, double max_degree,
+                            int lognormal, uint64_t seed);
 // host .mtx loader with the reference's rules; returns CSR in host vectors
 mg_status load_mtx_host(const char *path, uint32_t &n, std::vector<uint64_t> &off, std::vector<uint32_t> &cols,
                         std::vector<double> &w, std::string &err);

@@ -208,6 +208,22 @@ def test_generators_match_oracle(O, ctx):
     assert (off == g.offsets).all() and (cols == g.cols).all()
 
 
+def test_chunglu_generator_matches_oracle(O, ctx):
+    """Same topology as the oracle's Chung-Lu generator; lognormal weights equal
+    up to the device's and host's libm (float-rounded values, relative 1e-6)."""
+    for lognormal in (False, True):
+        dg = ctx.generate_chunglu(20000, 2.1, 20.0, 2000.0, lognormal=lognormal, seed=3)
+        g = O.gen_chunglu(20000, 2.1, 20.0, 2000.0, lognormal=lognormal, seed=3)
+        off, cols, w = dg.csr()
+        assert (off == g.offsets).all() and (cols == g.cols).all()
+        info = dg.info()
+        if lognormal:
+            assert np.allclose(w, g.weights, rtol=1e-6, atol=0)
+            assert not info["integral"]
+        else:
+            assert (w == 1.0).all() and info["integral"] and info["mass"] == g.nnz
+
+
 def test_mtx_loader_matches_oracle(O, ctx, tmp_path):
     g = O.gen_sbm(3000, 10, 8.0, 0.8, seed=6)
     row = np.repeat(np.arange(g.n), np.diff(g.offsets).astype(np.int64))
