@@ -267,3 +267,34 @@ def test_empty_and_edge_cases(O, ctx):
         ctx.graph_from_csr(3, np.array([0, 1, 2, 3], np.uint64), np.array([0, 5, 1], np.uint32))
     with pytest.raises(mg.MGError):
         _up(ctx, g).coarsen(np.array([0, 7], np.uint32))
+
+
+def _permute_rows(g, rng, duplicate=0.0):
+    """Same graph with every row's entries shuffled, optionally with some
+    (symmetric) entries listed twice."""
+    off = g.offsets.astype(np.int64)
+    src = np.repeat(np.arange(g.n), np.diff(off))
+    u, v = src, g.cols.astype(np.int64)
+    keep = u < v
+    u, v = u[keep], v[keep]
+    if duplicate:
+        d = rng.random(len(u)) < duplicate
+        u, v = np.concatenate([u, u[d]]), np.concatenate([v, v[d]])
+    a, b = np.concatenate([u, v]), np.concatenate([v, u])
+    order = np.lexsort((rng.random(len(a)), a))
+    a, b = a[order], b[order]
+    offs = np.zeros(g.n + 1, np.uint64)
+    np.add.at(offs, a + 1, 1)
+    return type(g)(g.n, np.cumsum(offs).astype(np.uint64), b.astype(np.uint32), None)
+
+
+@pytest.mark.parametrize("duplicate", [0.0, 0.05])
+def test_unsorted_and_repeated_columns(O, ctx, duplicate):
+    """Rows that are not sorted (shuffled) or list an edge twice (parallel
+    edges, summed into k_ic like any repeated community): results stay exact."""
+    rng = np.random.default_rng(17)
+    for base in (O.gen_rmat(13, seed=4), O.gen_sbm(6000, 32, 14.0, 0.8, seed=5)):
+        g = _permute_rows(base, rng, duplicate)
+        a = _up(ctx, g).louvain()
+        b = O.louvain(g)
+        _compare_runs(a, b)
