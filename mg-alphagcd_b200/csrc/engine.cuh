@@ -148,6 +148,13 @@ struct SweepParams {
     int precision = MG_PREC_FP64;
     double mass = 0;
     int integral = 0;
+    // combine neighbours of equal community inside a warp before inserting
+    // into the cluster tables (integral weights), where many threads of a
+    // heavy vertex otherwise add to the same slot.  Pays when many neighbours
+    // share communities;
+    // set from the previous sweep's distinct candidates per edge (never on the
+    // first sweep of a phase, where every community is one vertex).
+    int agg = 0;
 };
 
 // Constants of the gain of one graph, from its mass (sum of all directed

@@ -28,6 +28,7 @@ struct LMArgs {
     GainK K;             // gain constants of the graph
     int up;
     int integral;
+    int agg;             // combine equal communities in the warp before inserting (cluster tables)
     SweepAcc *acc;
     // batched sweeps: graph of each vertex, per-graph control word and gain
     // constants, the three assignment buffers, sum_in per vertex, and the
@@ -604,7 +605,10 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
         const double ki = A.k[i];
         const double a = A.sigma[src] - ki;
         double e_part = 0, s_part = 0;
-        for (uint32_t base = lo + tc; base < hi; base += stride * BATCH) {
+        // a warp-uniform loop bound (lanes past the row's end take part with no
+        // edge), so that the warp can combine equal communities below
+        for (uint32_t wbase = lo + (tc & ~31u); wbase < hi; wbase += stride * BATCH) {
+            const uint32_t base = wbase + (tc & 31u);
             uint32_t jj[BATCH], cc[BATCH];
             double ww[BATCH];
 #pragma unroll
@@ -617,75 +621,85 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
             for (int b = 0; b < BATCH; b++) cc[b] = jj[b] != kEmpty ? vv.P[jj[b]] : kEmpty;
 #pragma unroll
             for (int b = 0; b < BATCH; b++) {
-                if (jj[b] == kEmpty) continue;
                 const uint32_t c = cc[b];
-                if (c != src) {
-                    if (!is_candidate<VER>(c, src, up)) continue;
+                const bool cand = jj[b] != kEmpty && c != src && is_candidate<VER>(c, src, up);
+                if (jj[b] != kEmpty && c == src) {
+                    if (jj[b] != i) e_part += ww[b];
+                    else s_part += ww[b];
+                }
+                if constexpr (kIntg<WK>) {
+                    // lanes holding the same community add their weights in the
+                    // warp; one leader per community inserts the sum (integer
+                    // sums: the result does not depend on the grouping)
+                    uint32_t wsum = cand ? (uint32_t)ww[b] : 0u;
+                    bool lead = cand;
+                    if (A.agg) {  // uniform: a kernel argument
+                        const uint32_t peers = __match_any_sync(0xffffffffu, cand ? c : kEmpty);
+                        wsum = __reduce_add_sync(peers, wsum);
+                        lead = cand && (uint32_t)(__ffs(peers) - 1) == (threadIdx.x & 31u);
+                    }
+                    if (!lead) continue;
                     const uint32_t h = hash_range(c, (uint32_t)CS * S);
                     const unsigned owner = h / S;
                     uint32_t s = h & (S - 1);
-                    if constexpr (kIntg<WK>) {
-                        const unsigned long long wi = (uint32_t)ww[b];
-                        uint64_t *seg = rank_ptr<CS>(packed, owner);
-                        bool placed = false;
-                        for (int p = 0; p < S; p++) {
-                            uint64_t cur = ((volatile uint64_t *)seg)[s];
-                            uint32_t k = (uint32_t)(cur >> 32);
-                            if (k == c) {
+                    const unsigned long long wi = wsum;
+                    uint64_t *seg = rank_ptr<CS>(packed, owner);
+                    bool placed = false;
+                    for (int p = 0; p < S; p++) {
+                        uint64_t cur = ((volatile uint64_t *)seg)[s];
+                        uint32_t k = (uint32_t)(cur >> 32);
+                        if (k == c) {
+                            atomicAdd((unsigned long long *)(seg + s), wi);
+                            placed = true;
+                            break;
+                        }
+                        if (k == kEmpty) {
+                            uint64_t prev = atomicCAS((unsigned long long *)(seg + s), kEmpty64, ((uint64_t)c << 32) | wi);
+                            if (prev == kEmpty64) {
+                                rank_ptr<CS>(used, owner)[atomicAdd(rank_ptr<CS>(&ucnt, owner), 1u)] = (uint16_t)s;
+                                placed = true;
+                                break;
+                            }
+                            if ((uint32_t)(prev >> 32) == c) {
                                 atomicAdd((unsigned long long *)(seg + s), wi);
                                 placed = true;
                                 break;
                             }
-                            if (k == kEmpty) {
-                                uint64_t prev = atomicCAS((unsigned long long *)(seg + s), kEmpty64,
-                                                          ((uint64_t)c << 32) | wi);
-                                if (prev == kEmpty64) {
-                                    rank_ptr<CS>(used, owner)[atomicAdd(rank_ptr<CS>(&ucnt, owner), 1u)] =
-                                        (uint16_t)s;
-                                    placed = true;
-                                    break;
-                                }
-                                if ((uint32_t)(prev >> 32) == c) {
-                                    atomicAdd((unsigned long long *)(seg + s), wi);
-                                    placed = true;
-                                    break;
-                                }
-                            }
-                            s = (s + 1) & (S - 1);
                         }
-                        if (!placed) atomicAdd(&A.acc->overflow, 1ull);
-                    } else {
-                        uint32_t *ks = rank_ptr<CS>(keys, owner);
-                        double *vs = rank_ptr<CS>(vals, owner);
-                        bool placed = false;
-                        for (int p = 0; p < S; p++) {
-                            uint32_t cur = ((volatile uint32_t *)ks)[s];
-                            if (cur == c) {
+                        s = (s + 1) & (S - 1);
+                    }
+                    if (!placed) atomicAdd(&A.acc->overflow, 1ull);
+                } else {
+                    if (!cand) continue;
+                    const uint32_t h = hash_range(c, (uint32_t)CS * S);
+                    const unsigned owner = h / S;
+                    uint32_t s = h & (S - 1);
+                    uint32_t *ks = rank_ptr<CS>(keys, owner);
+                    double *vs = rank_ptr<CS>(vals, owner);
+                    bool placed = false;
+                    for (int p = 0; p < S; p++) {
+                        uint32_t cur = ((volatile uint32_t *)ks)[s];
+                        if (cur == c) {
+                            placed = true;
+                            break;
+                        }
+                        if (cur == kEmpty) {
+                            uint32_t prev = atomicCAS(ks + s, kEmpty, c);
+                            if (prev == kEmpty) {
+                                rank_ptr<CS>(used, owner)[atomicAdd(rank_ptr<CS>(&ucnt, owner), 1u)] =
+                                    (uint16_t)s;
                                 placed = true;
                                 break;
                             }
-                            if (cur == kEmpty) {
-                                uint32_t prev = atomicCAS(ks + s, kEmpty, c);
-                                if (prev == kEmpty) {
-                                    rank_ptr<CS>(used, owner)[atomicAdd(rank_ptr<CS>(&ucnt, owner), 1u)] =
-                                        (uint16_t)s;
-                                    placed = true;
-                                    break;
-                                }
-                                if (prev == c) {
-                                    placed = true;
-                                    break;
-                                }
+                            if (prev == c) {
+                                placed = true;
+                                break;
                             }
-                            s = (s + 1) & (S - 1);
                         }
-                        if (placed) atomicAdd(vs + s, ww[b]);
-                        else atomicAdd(&A.acc->overflow, 1ull);
+                        s = (s + 1) & (S - 1);
                     }
-                } else if (jj[b] != i) {
-                    e_part += ww[b];
-                } else {
-                    s_part += ww[b];
+                    if (placed) atomicAdd(vs + s, ww[b]);
+                    else atomicAdd(&A.acc->overflow, 1ull);
                 }
             }
         }

@@ -23,6 +23,7 @@ LMArgs batch_args(const GraphView &g, MoveWorkspace &ws, const SweepParams &p, c
     A.perm = b.perm;
     A.pgid = b.pgid;
     A.integral = p.integral;
+    A.agg = p.agg;
     A.acc = ws.acc.ensure(1);
     A.gid = b.gid;
     A.gword = b.gword;

@@ -113,6 +113,7 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
         int base = 0, pend = 1;
         // first sweep: P = identity (base), proposes C[1]; yields Q0
         sp.up = 1;
+        sp.agg = 0;
         // shapes of the light classes (autotuner; its timing runs write the
         // proposal this sweep writes)
         move_tune(cur, mlv, ctx->mws, sp, C[base], C[pend], k, sigma, s);
@@ -138,6 +139,9 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
         int loop = 0;
         while (true) {
             sp.up = !sp.up;
+            // combine equal communities in the warp once they repeat: fewer
+            // than half of the last sweep's edges were distinct candidates
+            sp.agg = 2 * hacc.distinct < cur.nnz;
             const int next = 3 - base - pend;
             Timer ti(ctx->ev[0], ctx->ev[1], s);
             sweep_reset_acc(ctx->mws, s);
