@@ -532,13 +532,14 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
 }
 
 // ============================================================================
-// bin 9, tiers 0-4: one vertex per thread-block cluster of CS CTAs, the
-// cluster's distributed shared memory holding one hash table of CS *
-// kClusterSlots slots.  A neighbour community hashes to (owner CTA, slot);
-// inserts into other CTAs' segments go through DSMEM atomics; each CTA then
-// evaluates the candidates of its own segment, and rank 0 reduces the CS
-// winners.  Two cluster barriers per vertex (accumulators double-buffered).
-// Unit weights use packed 64-bit slots {key:32 | count:32}.
+// classes 13-17: one vertex per thread-block cluster of CS CTAs, the
+// cluster's shared memory holding one hash table of CS * kClusterSlots slots.
+// A neighbour community hashes to (owner CTA, slot); the owner's segment
+// collects its sum (see the two fill modes below), each CTA evaluates the
+// candidates of its segment, and rank 0 reduces the CS winners through
+// distributed shared memory.  Two cluster barriers per
+// vertex (accumulators double-buffered).  Integral weights use packed 64-bit
+// slots {key:32 | sum:32}.
 // ============================================================================
 namespace cg = cooperative_groups;
 constexpr int kClusterThreads = 1024;  // one CTA per SM with a 16K-slot segment
@@ -591,8 +592,6 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
     if (threadIdx.x == 0) ucnt = 0;
     cluster_barrier<CS>();
     const uint32_t cluster_id = blockIdx.x / CS, nclusters = gridDim.x / CS;
-    const uint32_t tc = rank * kClusterThreads + threadIdx.x;
-    constexpr uint32_t stride = CS * kClusterThreads;
     double sin = 0;
     unsigned dcnt = 0;
     int par = 0;
@@ -605,16 +604,26 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
         const double ki = A.k[i];
         const double a = A.sigma[src] - ki;
         double e_part = 0, s_part = 0;
-        // a warp-uniform loop bound (lanes past the row's end take part with no
-        // edge), so that the warp can combine equal communities below
-        for (uint32_t wbase = lo + (tc & ~31u); wbase < hi; wbase += stride * BATCH) {
-            const uint32_t base = wbase + (tc & 31u);
+        // Two ways to fill the cluster's table, chosen per sweep:
+        //  * distinct-heavy sweeps (no combining): every CTA reads the whole row
+        //    (it stays in cache) and inserts only the communities whose slots
+        //    it owns, so all table atomics are local;
+        //  * sweeps where communities repeat (A.agg): the CTAs split the row,
+        //    the warp combines equal communities, and the few remaining
+        //    inserts go to the owner CTA through distributed shared memory.
+        // The loop bound is warp-uniform (lanes past the row's end take part
+        // with no edge), so that the warp can combine equal communities.
+        const bool own = CS > 1 && !A.agg;
+        const uint32_t t0 = own ? threadIdx.x : rank * kClusterThreads + threadIdx.x;
+        const uint32_t step = own ? kClusterThreads : CS * kClusterThreads;
+        for (uint32_t wbase = lo + (t0 & ~31u); wbase < hi; wbase += step * BATCH) {
+            const uint32_t base = wbase + (t0 & 31u);
             uint32_t jj[BATCH], cc[BATCH];
             double ww[BATCH];
 #pragma unroll
             for (int b = 0; b < BATCH; b++) {
-                uint32_t e = base + b * stride;
-                jj[b] = e < hi ? __ldcs(A.col + e) : kEmpty;
+                uint32_t e = base + b * step;
+                jj[b] = e < hi ? (own ? __ldg(A.col + e) : __ldcs(A.col + e)) : kEmpty;
                 ww[b] = e < hi ? wload<WK>(A.w, e) : 0.0;
             }
 #pragma unroll
@@ -622,8 +631,16 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
 #pragma unroll
             for (int b = 0; b < BATCH; b++) {
                 const uint32_t c = cc[b];
-                const bool cand = jj[b] != kEmpty && c != src && is_candidate<VER>(c, src, up);
-                if (jj[b] != kEmpty && c == src) {
+                uint32_t s = 0;
+                unsigned owner = 0;
+                bool cand = jj[b] != kEmpty && c != src && is_candidate<VER>(c, src, up);
+                if (cand) {
+                    const uint32_t h = hash_range(c, (uint32_t)CS * S);
+                    owner = h / S;
+                    s = h & (S - 1);
+                    if (own) cand = owner == rank;
+                }
+                if ((!own || rank == 0) && jj[b] != kEmpty && c == src) {
                     if (jj[b] != i) e_part += ww[b];
                     else s_part += ww[b];
                 }
@@ -639,11 +656,10 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
                         lead = cand && (uint32_t)(__ffs(peers) - 1) == (threadIdx.x & 31u);
                     }
                     if (!lead) continue;
-                    const uint32_t h = hash_range(c, (uint32_t)CS * S);
-                    const unsigned owner = h / S;
-                    uint32_t s = h & (S - 1);
                     const unsigned long long wi = wsum;
-                    uint64_t *seg = rank_ptr<CS>(packed, owner);
+                    uint64_t *seg = own ? packed : rank_ptr<CS>(packed, owner);
+                    uint16_t *useg = own ? used : rank_ptr<CS>(used, owner);
+                    uint32_t *uc = own ? &ucnt : rank_ptr<CS>(&ucnt, owner);
                     bool placed = false;
                     for (int p = 0; p < S; p++) {
                         uint64_t cur = ((volatile uint64_t *)seg)[s];
@@ -656,7 +672,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
                         if (k == kEmpty) {
                             uint64_t prev = atomicCAS((unsigned long long *)(seg + s), kEmpty64, ((uint64_t)c << 32) | wi);
                             if (prev == kEmpty64) {
-                                rank_ptr<CS>(used, owner)[atomicAdd(rank_ptr<CS>(&ucnt, owner), 1u)] = (uint16_t)s;
+                                useg[atomicAdd(uc, 1u)] = (uint16_t)s;
                                 placed = true;
                                 break;
                             }
@@ -671,11 +687,10 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
                     if (!placed) atomicAdd(&A.acc->overflow, 1ull);
                 } else {
                     if (!cand) continue;
-                    const uint32_t h = hash_range(c, (uint32_t)CS * S);
-                    const unsigned owner = h / S;
-                    uint32_t s = h & (S - 1);
-                    uint32_t *ks = rank_ptr<CS>(keys, owner);
-                    double *vs = rank_ptr<CS>(vals, owner);
+                    uint32_t *ks = own ? keys : rank_ptr<CS>(keys, owner);
+                    double *vs = own ? vals : rank_ptr<CS>(vals, owner);
+                    uint16_t *useg = own ? used : rank_ptr<CS>(used, owner);
+                    uint32_t *uc = own ? &ucnt : rank_ptr<CS>(&ucnt, owner);
                     bool placed = false;
                     for (int p = 0; p < S; p++) {
                         uint32_t cur = ((volatile uint32_t *)ks)[s];
@@ -686,8 +701,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
                         if (cur == kEmpty) {
                             uint32_t prev = atomicCAS(ks + s, kEmpty, c);
                             if (prev == kEmpty) {
-                                rank_ptr<CS>(used, owner)[atomicAdd(rank_ptr<CS>(&ucnt, owner), 1u)] =
-                                    (uint16_t)s;
+                                useg[atomicAdd(uc, 1u)] = (uint16_t)s;
                                 placed = true;
                                 break;
                             }
