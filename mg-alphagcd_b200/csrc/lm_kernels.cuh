@@ -434,7 +434,11 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
         const int tb = table_bits(hi - lo, slots_log2);
         const uint32_t mask = (1u << tb) - 1u;
         V e_part = V(0), s_part = V(0);
-        for (uint32_t base = lo + t; base < hi; base += GT * BATCH) {
+        // warp-uniform loop bound (lanes past the row's end take part with no
+        // edge), so that the warp can append its new slots with one atomic
+        const uint32_t lane = threadIdx.x & 31u;
+        for (uint32_t wbase = lo + (t & ~31u); wbase < hi; wbase += GT * BATCH) {
+            const uint32_t base = wbase + lane;
             uint32_t jj[BATCH], cc[BATCH];
             V ww[BATCH];
 #pragma unroll
@@ -447,29 +451,41 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
             for (int b = 0; b < BATCH; b++) cc[b] = jj[b] != kEmpty ? vv.P[jj[b]] : kEmpty;
 #pragma unroll
             for (int b = 0; b < BATCH; b++) {
-                if (jj[b] == kEmpty) continue;
                 const uint32_t c = cc[b];
-                if (c != src) {
-                    if (!is_candidate<VER>(c, src, up)) continue;
-                    uint32_t h = hash_slot(c, tb);
-                    for (uint32_t p = 0; p < S; p++) {
-                        const uint32_t cur = ((volatile uint32_t *)keys)[h];
-                        if (cur == c) break;
-                        if (cur == kEmpty) {
-                            const uint32_t prev = atomicCAS(keys + h, kEmpty, c);
-                            if (prev == kEmpty) {
-                                used[atomicAdd(cnt + g, 1u)] = (uint16_t)h;
-                                break;
+                uint32_t hnew = kEmpty;  // slot this lane claimed for a new key
+                if (jj[b] != kEmpty) {
+                    if (c != src) {
+                        if (is_candidate<VER>(c, src, up)) {
+                            uint32_t h = hash_slot(c, tb);
+                            for (uint32_t p = 0; p < S; p++) {
+                                const uint32_t cur = ((volatile uint32_t *)keys)[h];
+                                if (cur == c) break;
+                                if (cur == kEmpty) {
+                                    const uint32_t prev = atomicCAS(keys + h, kEmpty, c);
+                                    if (prev == kEmpty) {
+                                        hnew = h;
+                                        break;
+                                    }
+                                    if (prev == c) break;
+                                }
+                                h = (h + 1) & mask;
                             }
-                            if (prev == c) break;
+                            atomicAdd(vals + h, ww[b]);
                         }
-                        h = (h + 1) & mask;
+                    } else if (jj[b] != i) {
+                        e_part += ww[b];
+                    } else {
+                        s_part += ww[b];
                     }
-                    atomicAdd(vals + h, ww[b]);
-                } else if (jj[b] != i) {
-                    e_part += ww[b];
-                } else {
-                    s_part += ww[b];
+                }
+                // the warp's new slots join the table's list with one atomic
+                const uint32_t m = __ballot_sync(0xffffffffu, hnew != kEmpty);
+                if (m) {
+                    const uint32_t leader = __ffs(m) - 1;
+                    uint32_t pos = 0;
+                    if (lane == leader) pos = atomicAdd(cnt + g, (uint32_t)__popc(m));
+                    pos = __shfl_sync(0xffffffffu, pos, leader);
+                    if (hnew != kEmpty) used[pos + __popc(m & ((1u << lane) - 1u))] = (uint16_t)hnew;
                 }
             }
         }
