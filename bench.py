@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--batch-steps", type=int, default=2)
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the sbm64k and precision lines")
+    ap.add_argument("--tune", choices=["on", "cached", "off"], default="on",
+                    help="autotuner of the kernel shapes per degree class (on: time new classes)")
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     return ap.parse_args()
@@ -401,6 +403,7 @@ def run_serving(mg, args, local):
 def run_engine(args, world, rank, local, pg):
     mg = importlib.import_module("mg-alphagcd_b200")
     ctx = mg.Context(local)
+    ctx.tune_mode({"on": mg.TUNE_ON, "cached": mg.TUNE_CACHED, "off": mg.TUNE_OFF}[args.tune])
     g = ctx.generate_rmat(args.scale, RMAT["edge_factor"], RMAT["a"], RMAT["b"], RMAT["c"], RMAT["seed"])
     info = g.info()
     for _ in range(max(args.warmup, 0)):

@@ -394,8 +394,10 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
     V *vals_all = (V *)smem_raw;
     uint32_t *keys_all = (uint32_t *)(smem_raw + sizeof(V) * S * GPB);
     uint16_t *used_all = (uint16_t *)(smem_raw + (sizeof(V) + sizeof(uint32_t)) * S * GPB);
-    __shared__ V acc_e[GPB], acc_s[GPB];
-    __shared__ uint32_t cnt[GPB];
+    // per-vertex sums and candidate counters, double-buffered by the parity
+    // of the group's vertex: the next vertex starts before they are cleared
+    __shared__ V acc_e[2][GPB], acc_s[2][GPB];
+    __shared__ uint32_t cnt[2][GPB];
     __shared__ G red_g[32];
     __shared__ uint32_t red_c[32];
     const int g = threadIdx.x / GT, t = threadIdx.x % GT;
@@ -407,14 +409,17 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
         vals_all[s2] = V(0);
     }
     if (threadIdx.x < GPB) {
-        acc_e[threadIdx.x] = V(0);
-        acc_s[threadIdx.x] = V(0);
-        cnt[threadIdx.x] = 0;
+        for (int q = 0; q < 2; q++) {
+            acc_e[q][threadIdx.x] = V(0);
+            acc_s[q][threadIdx.x] = V(0);
+            cnt[q][threadIdx.x] = 0;
+        }
     }
     __syncthreads();
     double sin = 0;
     unsigned dcnt = 0;
-    for (uint32_t idx = blockIdx.x * GPB + g; idx - g < bin_size; idx += gridDim.x * GPB) {
+    int par = 0;
+    for (uint32_t idx = blockIdx.x * GPB + g; idx - g < bin_size; idx += gridDim.x * GPB, par ^= 1) {
         // the loop condition is uniform inside a group (GT == 32) or block (GT > 32)
         bool active = idx < bin_size;
         uint32_t i = 0, src = 0, lo = 0, hi = 0;
@@ -483,7 +488,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
                 if (m) {
                     const uint32_t leader = __ffs(m) - 1;
                     uint32_t pos = 0;
-                    if (lane == leader) pos = atomicAdd(cnt + g, (uint32_t)__popc(m));
+                    if (lane == leader) pos = atomicAdd(&cnt[par][g], (uint32_t)__popc(m));
                     pos = __shfl_sync(0xffffffffu, pos, leader);
                     if (hnew != kEmpty) used[pos + __popc(m & ((1u << lane) - 1u))] = (uint16_t)hnew;
                 }
@@ -494,12 +499,12 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
         e_part = warp_sum(e_part);
         s_part = warp_sum(s_part);
         if ((threadIdx.x & 31) == 0) {
-            if (e_part != V(0)) atomicAdd(acc_e + g, e_part);
-            if (s_part != V(0)) atomicAdd(acc_s + g, s_part);
+            if (e_part != V(0)) atomicAdd(&acc_e[par][g], e_part);
+            if (s_part != V(0)) atomicAdd(&acc_s[par][g], s_part);
         }
         group_sync<GT>();
-        const double e_src = v2d(acc_e[g]), selfw = v2d(acc_s[g]);
-        const uint32_t nd = cnt[g];
+        const double e_src = v2d(acc_e[par][g]), selfw = v2d(acc_s[par][g]);
+        const uint32_t nd = cnt[par][g];
         G best = G(0);
         uint32_t dst = src;
         for (uint32_t u0 = t; u0 < nd; u0 += GT * EB) {
@@ -531,18 +536,48 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
                 }
             }
         }
-        group_argmax<GT, G>(best, dst, up, red_g, red_c);
+        // argmax over the group: warp shuffles, then (wider groups) the
+        // warps' winners meet in shared memory behind one barrier and thread 0
+        // of the group takes the best.  The table was cleaned during the
+        // evaluation, before that barrier, so the next vertex may start.
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            G g2 = shfl_xor_g(best, o);
+            uint32_t c2 = __shfl_xor_sync(0xffffffffu, dst, o);
+            if (better(g2, c2, best, dst, up)) {
+                best = g2;
+                dst = c2;
+            }
+        }
+        if constexpr (GT > 32) {
+            const int warp = threadIdx.x >> 5;
+            if ((threadIdx.x & 31) == 0) {
+                red_g[warp] = best;
+                red_c[warp] = dst;
+            }
+            __syncthreads();
+            if (t == 0) {
+#pragma unroll
+                for (int w2 = 1; w2 < GT / 32; w2++) {
+                    if (better(red_g[warp + w2], red_c[warp + w2], best, dst, up)) {
+                        best = red_g[warp + w2];
+                        dst = red_c[warp + w2];
+                    }
+                }
+            }
+        }
         if (t == 0) {
             if (active) {
                 vv.N[i] = final_choice<VER>(dst, src, up);
                 put_sin<BT>(A, i, sin, e_src + selfw);
                 dcnt += nd;
             }
-            cnt[g] = 0;
-            acc_e[g] = V(0);
-            acc_s[g] = V(0);
+            // used again two vertices on, after at least one more barrier
+            cnt[par][g] = 0;
+            acc_e[par][g] = V(0);
+            acc_s[par][g] = V(0);
         }
-        group_sync<GT>();
+        if constexpr (GT == 32) __syncwarp();
     }
     flush_acc(A.acc, A.integral, sin, dcnt);
 }
