@@ -22,7 +22,9 @@ the community count of every level) and "precision" (seeded Chung-Lu graph,
 4,194,304 vertices, exponent 2.1, mean degree 20, degrees capped at 200,000,
 float lognormal(0, 1) weights: FP32 gains against FP64 gains, the FP64
 modularity recomputed from the FP32 run's assignment, and exact int64 gains
-against FP64 gains on the unit-weight copy of the same graph).
+against FP64 gains on the unit-weight copy of the same graph).  "loader"
+times the host Matrix Market loader on an R-MAT-20 file: parse, parse with
+the binary CSR cache written, load from the cache, and a graph built from it.
 
 It also carries "serving": a Poisson stream of Louvain jobs (default 200
 requests/s for 60 s; half SBM, half R-MAT with edge factor 16 and the
@@ -283,6 +285,62 @@ def run_precision(ctx):
                              "same_assignment": bool((ui[-1]["assignment"] == u64[-1]["assignment"]).all())}}
 
 
+def run_loader(mg, ctx, scale=20):
+    """Host .mtx loader: an R-MAT-20 graph written as a symmetric pattern
+    Matrix Market file, then parsed (mmap, all host threads), parsed with the
+    binary CSR cache written, loaded from that cache, and uploaded from it."""
+    import shutil
+    import tempfile
+
+    import numpy as np
+    import pandas as pd
+
+    g = ctx.generate_rmat(scale, RMAT["edge_factor"], RMAT["a"], RMAT["b"], RMAT["c"], RMAT["seed"])
+    off, cols, _ = g.csr()
+    g.close()
+    n = len(off) - 1
+    row = np.repeat(np.arange(n, dtype=np.int64), np.diff(off.astype(np.int64)))
+    m = row > cols
+    d = tempfile.mkdtemp(prefix="mgload")
+    try:
+        path = os.path.join(d, f"rmat{scale}.mtx")
+        with open(path, "w") as f:
+            f.write("%%MatrixMarket matrix coordinate pattern symmetric\n")
+            f.write(f"{n} {n} {int(m.sum())}\n")
+        pd.DataFrame({"r": row[m] + 1, "c": cols[m].astype(np.int64) + 1}).to_csv(
+            path, mode="a", sep=" ", header=False, index=False)
+        size = os.path.getsize(path)
+        del row, m
+        L = mg.lib()
+        import ctypes as ct
+
+        def timed(flags):
+            h = ct.c_void_p()
+            t0 = time.perf_counter()
+            st = L.mg_csr_from_mtx(path.encode(), flags, ct.byref(h))
+            t = time.perf_counter() - t0
+            L.mg_csr_free(h)
+            if st != 0:
+                raise RuntimeError(f"mg_csr_from_mtx: status {st}")
+            return t
+
+        parse = min(timed(0) for _ in range(3))
+        write = timed(mg.LOAD_CACHE_WRITE)
+        cached = min(timed(mg.LOAD_CACHE_READ) for _ in range(3))
+        t0 = time.perf_counter()
+        h = ctx.graph_from_mtx(path, cache_read=True)
+        up = time.perf_counter() - t0
+        same = bool((h.csr()[1] == cols).all())
+        h.close()
+        return {"workload": f"R-MAT-{scale} (edge factor 16) as a symmetric pattern .mtx, {size / 1e6:.0f} MB, "
+                            f"{len(cols)} directed entries", "threads": os.cpu_count(),
+                "parse_s": parse, "parse_mb_per_s": size / 1e6 / parse, "parse_entries_per_s": len(cols) / parse,
+                "parse_and_cache_write_s": write, "cache_load_s": cached,
+                "graph_from_cache_s": up, "graph_equals_generator": same}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
 BATCH = dict(n_range=(1000, 200000), blocks_range=(4, 256), deg_range=(8.0, 32.0), intra_range=(0.7, 0.9), seed=4)
 
 
@@ -456,11 +514,12 @@ def run_engine(args, world, rank, local, pg):
                "sample": f"one phase-0 sweep (local move + sigma update + modularity) over the same graph, "
                          f"{ct_:.1f} s on {threads} threads"}
         del csr
-    batched = serving = sbm64k = precision = None
+    batched = serving = sbm64k = precision = loader = None
     if world == 1 and not args.no_extra:
         g.close()
         sbm64k = run_sbm64k(ctx)
         precision = run_precision(ctx)
+        loader = run_loader(mg, ctx)
     if world == 1 and not args.no_batched:
         g.close()
         batched = run_batched(mg, ctx, args)
@@ -496,6 +555,7 @@ def run_engine(args, world, rank, local, pg):
         "gpu_launches": int(sum(r["kernel_launches"] for r in runs)),
         "sbm64k": sbm64k,
         "precision": precision,
+        "loader": loader,
         "batched": batched,
         "serving": serving,
     }

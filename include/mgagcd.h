@@ -84,6 +84,34 @@ mg_status mg_graph_from_device_csr(mg_ctx *ctx, uint32_t n, uint64_t nnz, const 
  * Replaces loadMMSparseMatrix / init_data_from_mtx (src/mmio/mmio_wrapper.cu:76-301). */
 mg_status mg_graph_from_mtx(mg_ctx *ctx, const char *path, mg_graph **out);
 
+/* ---- host-side loading (no GPU needed) ------------------------------------ */
+
+/* A symmetric CSR in host memory produced by the .mtx loader. */
+typedef struct mg_host_csr mg_host_csr;
+
+enum {
+    MG_LOAD_CACHE_READ = 1,  /* use "<path>.mgcsr" when it matches the file's size and mtime */
+    MG_LOAD_CACHE_WRITE = 2  /* write "<path>.mgcsr" after parsing (a failed write is not an error) */
+};
+
+/* Parse a Matrix Market file with the same rules as mg_graph_from_mtx
+ * (src/mmio/mmio_wrapper.cu:76-295): memory-mapped, parsed by all host
+ * threads, rows in file order.  Symmetric files give unit weights (the
+ * reference forces 1.0, :141-142) and no weight array. */
+mg_status mg_csr_from_mtx(const char *path, int flags, mg_host_csr **out);
+/* Sizes; weighted = 0 when every weight is 1; from_cache = 1 when the arrays
+ * were mapped from the binary cache; cache_written = 1 when this load wrote it.
+ * Any pointer may be NULL. */
+mg_status mg_csr_info(const mg_host_csr *c, uint32_t *n, uint64_t *nnz, int *weighted, int *from_cache,
+                      int *cache_written);
+/* Borrowed views, valid until mg_csr_free: offsets[n+1], cols[nnz], weights[nnz] (NULL when unweighted). */
+mg_status mg_csr_arrays(const mg_host_csr *c, const uint64_t **offsets, const uint32_t **cols,
+                        const double **weights);
+void mg_csr_free(mg_host_csr *c);
+
+/* mg_graph_from_mtx with cache flags (MG_LOAD_*). */
+mg_status mg_graph_from_mtx_ex(mg_ctx *ctx, const char *path, int flags, mg_graph **out);
+
 /* Seeded synthetic graphs generated on the device (integer-only RNG; the
  * same seed gives the same graph as the CPU generators of the test oracle).
  * Replaces HostGraph::randomly_generate_graph (src/graph/host_graph.cpp:38-77). */
@@ -171,6 +199,7 @@ typedef struct {
     int max_phases;    /* default 1000 (src/main.cu:23) */
     int precision;     /* MG_PREC_* */
     int verbose;       /* print the reference's per-phase tables */
+    int keep_levels;   /* keep the dendrogram: every level's community map (mg_result_level_map) */
 } mg_run_opts;
 
 typedef struct {
@@ -200,6 +229,14 @@ mg_status mg_result_summary(const mg_result *r, mg_summary *s);
 mg_status mg_result_assignment(const mg_result *r, uint32_t *out);
 /* vertex count at the start of each phase; *count receives the number */
 mg_status mg_result_level_sizes(const mg_result *r, uint32_t *out, int max, int *count);
+/* Dendrogram of a run with keep_levels = 1: the community map of level
+ * `level` (0 = the input graph), one id in [0, size of the next level) per
+ * vertex of that level.  Composing the maps of levels 0 .. count-1 gives
+ * mg_result_assignment; the reference keeps only its last level
+ * (src/louvain/louvain.cu:1674-1693).  *size = vertices of the level; `out`
+ * (may be NULL) receives min(size, max) entries.  MG_ERR_INVALID when the
+ * run did not keep levels or `level` is out of range. */
+mg_status mg_result_level_map(const mg_result *r, int level, uint32_t *out, uint32_t max, uint32_t *size);
 /* the reference's printed table as rows {phase, loop, Q, dQ} */
 mg_status mg_result_trace(const mg_result *r, double *rows4, int max_rows, int *count);
 mg_status mg_result_destroy(mg_result *r);

@@ -50,7 +50,7 @@ class _Opts(ct.Structure):
 
 class _RunOpts(ct.Structure):
     _fields_ = [("version", ct.c_int), ("threshold", ct.c_double), ("max_phases", ct.c_int),
-                ("precision", ct.c_int), ("verbose", ct.c_int)]
+                ("precision", ct.c_int), ("verbose", ct.c_int), ("keep_levels", ct.c_int)]
 
 
 class _Summary(ct.Structure):
@@ -115,8 +115,11 @@ EXPORTED = [
     "mg_serve_submit", "mg_serve_submit_csr", "mg_serve_poll", "mg_serve_wait", "mg_serve_assignment",
     "mg_serve_cancel", "mg_serve_release", "mg_serve_stats", "mg_serve_last_error", "mg_serve_stop",
     "mg_tune_mode", "mg_tune_table", "mg_tune_save", "mg_tune_load", "mg_graph_generate_chunglu",
+    "mg_graph_from_mtx_ex", "mg_csr_from_mtx", "mg_csr_info", "mg_csr_arrays", "mg_csr_free",
+    "mg_result_level_map",
 ]
 TUNE_OFF, TUNE_CACHED, TUNE_ON = 0, 1, 2
+LOAD_CACHE_READ, LOAD_CACHE_WRITE = 1, 2
 
 
 def lib():
@@ -140,6 +143,12 @@ def lib():
     L.mg_graph_from_csr.argtypes = [vp, u32, vp, vp, vp, i32, pp]
     L.mg_graph_from_device_csr.argtypes = [vp, u32, u64, vp, vp, vp, i32, pp]
     L.mg_graph_from_mtx.argtypes = [vp, ct.c_char_p, pp]
+    L.mg_graph_from_mtx_ex.argtypes = [vp, ct.c_char_p, i32, pp]
+    L.mg_csr_from_mtx.argtypes = [ct.c_char_p, i32, pp]
+    L.mg_csr_info.argtypes = [vp, ct.POINTER(u32), ct.POINTER(u64), ct.POINTER(i32), ct.POINTER(i32),
+                              ct.POINTER(i32)]
+    L.mg_csr_arrays.argtypes = [vp, pp, pp, pp]
+    L.mg_csr_free.argtypes = [vp]
     L.mg_graph_generate_rmat.argtypes = [vp, i32, i32, dbl, dbl, dbl, u64, pp]
     L.mg_graph_generate_sbm.argtypes = [vp, u32, u32, dbl, dbl, u64, pp]
     L.mg_graph_generate_chunglu.argtypes = [vp, u32, dbl, dbl, dbl, i32, u64, pp]
@@ -156,6 +165,7 @@ def lib():
     L.mg_result_assignment.argtypes = [vp, vp]
     L.mg_result_level_sizes.argtypes = [vp, vp, i32, ct.POINTER(i32)]
     L.mg_result_trace.argtypes = [vp, vp, i32, ct.POINTER(i32)]
+    L.mg_result_level_map.argtypes = [vp, i32, vp, u32, ct.POINTER(u32)]
     L.mg_result_destroy.argtypes = [vp]
     L.mg_batch_draw_sbm_params.argtypes = [u32, u32, u32, u32, u32, dbl, dbl, dbl, dbl, u64, vp]
     L.mg_batch_generate_sbm.argtypes = [vp, u32, vp, pp]
@@ -239,9 +249,15 @@ class Context:
                    "mg_graph_from_csr")
         return Graph(self, h)
 
-    def graph_from_mtx(self, path: str) -> "Graph":
+    def graph_from_mtx(self, path: str, cache_read: bool = False, cache_write: bool = False) -> "Graph":
+        """Load a Matrix Market file (mg_graph_from_mtx; with the binary CSR
+        cache flags, mg_graph_from_mtx_ex)."""
         h = ct.c_void_p()
-        self.check(lib().mg_graph_from_mtx(self.h, path.encode(), ct.byref(h)), "mg_graph_from_mtx")
+        flags = (LOAD_CACHE_READ if cache_read else 0) | (LOAD_CACHE_WRITE if cache_write else 0)
+        if flags:
+            self.check(lib().mg_graph_from_mtx_ex(self.h, path.encode(), flags, ct.byref(h)), "mg_graph_from_mtx_ex")
+        else:
+            self.check(lib().mg_graph_from_mtx(self.h, path.encode(), ct.byref(h)), "mg_graph_from_mtx")
         return Graph(self, h)
 
     def generate_rmat(self, scale: int, edge_factor: int = 16, a=0.57, b=0.19, c=0.19, seed: int = 2) -> "Graph":
@@ -446,6 +462,39 @@ class Server:
             pass
 
 
+def load_mtx(path: str, cache_read: bool = False, cache_write: bool = False) -> dict:
+    """Parse a Matrix Market file on the host (mg_csr_from_mtx; no GPU needed).
+
+    Returns {"n", "offsets" (uint64), "cols" (uint32), "weights" (float64 or
+    None for unit weights), "from_cache", "cache_written"}; the arrays are
+    copies."""
+    L = lib()
+    h = ct.c_void_p()
+    flags = (LOAD_CACHE_READ if cache_read else 0) | (LOAD_CACHE_WRITE if cache_write else 0)
+    st = L.mg_csr_from_mtx(path.encode(), flags, ct.byref(h))
+    if st != MG_OK:
+        raise MGError(st, L.mg_last_error(None).decode())
+    try:
+        n, nnz = ct.c_uint32(), ct.c_uint64()
+        wt, fc, cw = ct.c_int(), ct.c_int(), ct.c_int()
+        L.mg_csr_info(h, ct.byref(n), ct.byref(nnz), ct.byref(wt), ct.byref(fc), ct.byref(cw))
+        po, pc, pw = ct.c_void_p(), ct.c_void_p(), ct.c_void_p()
+        L.mg_csr_arrays(h, ct.byref(po), ct.byref(pc), ct.byref(pw))
+
+        def copy(ptr, count, ctype, dtype):
+            if count == 0:
+                return np.zeros(0, dtype)
+            return np.ctypeslib.as_array(ct.cast(ptr, ct.POINTER(ctype)), (count,)).astype(dtype, copy=True)
+
+        off = copy(po, n.value + 1, ct.c_uint64, np.uint64)
+        cols = copy(pc, nnz.value, ct.c_uint32, np.uint32)
+        w = copy(pw, nnz.value, ct.c_double, np.float64) if wt.value else None
+        return {"n": n.value, "offsets": off, "cols": cols, "weights": w, "from_cache": bool(fc.value),
+                "cache_written": bool(cw.value)}
+    finally:
+        L.mg_csr_free(h)
+
+
 def draw_sbm_params(graphs: int, n_range=(1000, 200000), blocks_range=(4, 256), deg_range=(8.0, 32.0),
                     intra_range=(0.7, 0.9), seed: int = 4) -> list:
     """Per-graph SBM parameters of a batch (mg_batch_draw_sbm_params)."""
@@ -589,8 +638,10 @@ class Graph:
         return cd[:n], Graph(self.ctx, h)
 
     def louvain(self, version: int = 2, threshold: float = 1e-6, max_phases: int = 1000,
-                precision: str = "fp64", verbose: bool = False) -> dict:
-        opts = _RunOpts(version, threshold, max_phases, _PREC[precision], int(verbose))
+                precision: str = "fp64", verbose: bool = False, keep_levels: bool = False) -> dict:
+        """mg_louvain_run; with keep_levels the result also holds "level_maps",
+        the dendrogram (one community map per level, mg_result_level_map)."""
+        opts = _RunOpts(version, threshold, max_phases, _PREC[precision], int(verbose), int(keep_levels))
         r = ct.c_void_p()
         self.ctx.check(lib().mg_louvain_run(self.h, ct.byref(opts), ct.byref(r)), "mg_louvain_run")
         try:
@@ -610,6 +661,16 @@ class Graph:
             out.update({"assignment": a[:n], "level_sizes": lv[: len(lv) if cnt.value else 0],
                         "trace": tr[: cnt.value]})
             out["level_sizes"] = lv[: s.levels]
+            if keep_levels:
+                maps = []
+                for lvl in range(s.levels):
+                    size = ct.c_uint32()
+                    if lib().mg_result_level_map(r, lvl, None, 0, ct.byref(size)) != MG_OK:
+                        break
+                    m = np.zeros(max(size.value, 1), np.uint32)
+                    lib().mg_result_level_map(r, lvl, _p(m), size.value, ct.byref(size))
+                    maps.append(m[: size.value])
+                out["level_maps"] = maps
             return out
         finally:
             lib().mg_result_destroy(r)

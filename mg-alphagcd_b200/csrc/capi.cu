@@ -7,6 +7,7 @@
 #include <new>
 
 #include "handles.cuh"
+#include "host_csr.h"
 
 using namespace mg;
 
@@ -162,22 +163,66 @@ mg_status mg_graph_from_device_csr(mg_ctx *ctx, uint32_t n, uint64_t nnz, const 
 }
 
 mg_status mg_graph_from_mtx(mg_ctx *ctx, const char *path, mg_graph **out) {
+    return mg_graph_from_mtx_ex(ctx, path, 0, out);
+}
+
+mg_status mg_graph_from_mtx_ex(mg_ctx *ctx, const char *path, int flags, mg_graph **out) {
     if (!ctx || !out || !path) return fail(ctx, MG_ERR_INVALID, "mg_graph_from_mtx: NULL argument");
     *out = nullptr;
-    uint32_t n = 0;
-    std::vector<uint64_t> off;
-    std::vector<uint32_t> cols;
-    std::vector<double> w;
+    mg_host_csr c;
     std::string err;
     mg_status st;
     try {
-        st = load_mtx_host(path, n, off, cols, w, err);
+        st = load_mtx_csr(path, flags, c, err);
     } catch (const std::bad_alloc &) {
         return fail(ctx, MG_ERR_OOM, "host allocation failed while loading");
     }
     if (st != MG_OK) return fail(ctx, st, "mg_graph_from_mtx: " + err);
-    return mg_graph_from_csr(ctx, n, off.data(), cols.data(), w.data(), MG_WEIGHT_F64, out);
+    return mg_graph_from_csr(ctx, c.n, c.off, c.cols, c.w, c.weighted ? MG_WEIGHT_F64 : MG_WEIGHT_UNIT, out);
 }
+
+mg_status mg_csr_from_mtx(const char *path, int flags, mg_host_csr **out) {
+    if (!out || !path) return fail(nullptr, MG_ERR_INVALID, "mg_csr_from_mtx: NULL argument");
+    *out = nullptr;
+    mg_host_csr *c = new (std::nothrow) mg_host_csr();
+    if (!c) return fail(nullptr, MG_ERR_OOM, "host allocation failed");
+    std::string err;
+    mg_status st;
+    try {
+        st = load_mtx_csr(path, flags, *c, err);
+    } catch (const std::bad_alloc &) {
+        st = MG_ERR_OOM;
+        err = "host allocation failed while loading";
+    }
+    if (st != MG_OK) {
+        delete c;
+        return fail(nullptr, st, "mg_csr_from_mtx: " + err);
+    }
+    *out = c;
+    return MG_OK;
+}
+
+mg_status mg_csr_info(const mg_host_csr *c, uint32_t *n, uint64_t *nnz, int *weighted, int *from_cache,
+                      int *cache_written) {
+    if (!c) return fail(nullptr, MG_ERR_INVALID, "mg_csr_info: NULL csr");
+    if (n) *n = c->n;
+    if (nnz) *nnz = c->nnz;
+    if (weighted) *weighted = c->weighted;
+    if (from_cache) *from_cache = c->from_cache;
+    if (cache_written) *cache_written = c->cache_written;
+    return MG_OK;
+}
+
+mg_status mg_csr_arrays(const mg_host_csr *c, const uint64_t **offsets, const uint32_t **cols,
+                        const double **weights) {
+    if (!c) return fail(nullptr, MG_ERR_INVALID, "mg_csr_arrays: NULL csr");
+    if (offsets) *offsets = c->off;
+    if (cols) *cols = c->cols;
+    if (weights) *weights = c->w;
+    return MG_OK;
+}
+
+void mg_csr_free(mg_host_csr *c) { delete c; }
 
 mg_status mg_graph_generate_rmat(mg_ctx *ctx, int scale, int edge_factor, double a, double b, double c, uint64_t seed,
                                  mg_graph **out) {
@@ -446,6 +491,7 @@ mg_status mg_louvain_run(mg_graph *g, const mg_run_opts *opts, mg_result **out) 
     o.max_phases = 1000;
     o.precision = MG_PREC_FP64;
     o.verbose = 0;
+    o.keep_levels = 0;
     if (opts) o = *opts;
     if (o.version < 0 || o.version > 2) return fail(ctx, MG_ERR_INVALID, "version must be 0, 1 or 2");
     if (o.precision < 0 || o.precision > 2) return fail(ctx, MG_ERR_INVALID, "unknown precision");
@@ -478,6 +524,14 @@ mg_status mg_result_level_sizes(const mg_result *r, uint32_t *out, int max, int 
     if (count) *count = c;
     if (out)
         for (int i = 0; i < c && i < max; i++) out[i] = r->level_sizes[i];
+    return MG_OK;
+}
+
+mg_status mg_result_level_map(const mg_result *r, int level, uint32_t *out, uint32_t max, uint32_t *size) {
+    if (!r || level < 0 || level >= (int)r->level_maps.size()) return MG_ERR_INVALID;
+    const std::vector<uint32_t> &m = r->level_maps[(size_t)level];
+    if (size) *size = (uint32_t)m.size();
+    if (out) memcpy(out, m.data(), sizeof(uint32_t) * std::min<size_t>(m.size(), max));
     return MG_OK;
 }
 
@@ -701,6 +755,7 @@ mg_status mg_batch_run(mg_batch *b, const mg_run_opts *opts, int flags, mg_batch
     o.max_phases = 1000;
     o.precision = MG_PREC_FP64;
     o.verbose = 0;
+    o.keep_levels = 0;
     if (opts) o = *opts;
     if (o.version < 0 || o.version > 2) return fail(ctx, MG_ERR_INVALID, "version must be 0, 1 or 2");
     if (o.precision < 0 || o.precision > 2) return fail(ctx, MG_ERR_INVALID, "unknown precision");

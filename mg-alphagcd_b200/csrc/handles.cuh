@@ -53,6 +53,7 @@ struct mg_result {
     std::vector<uint32_t> assignment;
     std::vector<uint32_t> level_sizes;
     std::vector<double> trace;  // rows of 4
+    std::vector<std::vector<uint32_t>> level_maps;  // dendrogram (keep_levels)
 };
 
 namespace mg {
@@ -131,9 +132,6 @@ void graph_generate_sbm(mg_graph *g, uint32_t n, uint32_t blocks, double mean_de
                         uint64_t seed);
 void graph_generate_chunglu(mg_graph *g, uint32_t n, double exponent, double mean_degree, double max_degree,
                             int lognormal, uint64_t seed);
-// host .mtx loader with the reference's rules; returns CSR in host vectors
-mg_status load_mtx_host(const char *path, uint32_t &n, std::vector<uint64_t> &off, std::vector<uint32_t> &cols,
-                        std::vector<double> &w, std::string &err);
 // Louvain
 void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result &res);
 // batched form

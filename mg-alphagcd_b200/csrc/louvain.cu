@@ -186,6 +186,10 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
         Timer tc(ctx->ev[0], ctx->ev[1], s);
         const uint32_t nn = relabel_dense(C[base], n, Cd, ctx->cws, s);
         gather_compose(assign, Cd, n0, s);
+        if (o.keep_levels) {
+            res.level_maps.emplace_back(n);
+            MG_CUDA(cudaMemcpyAsync(res.level_maps.back().data(), Cd, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
+        }
         communities = nn;
         if ((Qh - Qold) <= thr) {
             S.seconds_coarsen += tc.stop_sync();

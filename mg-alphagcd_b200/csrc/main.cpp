@@ -15,6 +15,7 @@
 //   -scale <int> -edge_factor <int> -blocks <int> -seed <int>
 //   -device <int>               CUDA device
 //   -dump_assignment <file>     write "vertex community" lines (1-based like .mtx)
+//   -csr_cache 0|1              read / write the binary CSR cache "<file>.mgcsr" (default 0)
 // The reference's random graph (dense, directed, unseeded rand(),
 // src/graph/host_graph.cpp:38-77) is replaced by the seeded generators.
 #include <algorithm>
@@ -61,6 +62,7 @@ int main(int argc, char **argv) {
     const long long seed = get_argval<long long>(b, e, "-seed", 1);
     const int device = get_argval<int>(b, e, "-device", 0);
     const std::string dump = get_argval<std::string>(b, e, "-dump_assignment", "");
+    const int csr_cache = get_argval<int>(b, e, "-csr_cache", 0);
 
     if (version < 0 || version > 2) {
         printf("the version is unsupported\n");
@@ -82,7 +84,7 @@ int main(int argc, char **argv) {
     std::string name;
     if (!path.empty()) {
         printf("loading graph...\n");
-        st = mg_graph_from_mtx(ctx, path.c_str(), &g);
+        st = mg_graph_from_mtx_ex(ctx, path.c_str(), csr_cache ? MG_LOAD_CACHE_READ | MG_LOAD_CACHE_WRITE : 0, &g);
         name = path;
     } else if (gen == "rmat") {
         st = mg_graph_generate_rmat(ctx, scale, ef, 0.57, 0.19, 0.19, (uint64_t)seed, &g);
@@ -110,7 +112,7 @@ int main(int argc, char **argv) {
     std::cout << std::setw(25) << name << std::setw(25) << n << std::setw(25) << nnz << std::endl;
     std::cout << std::setfill('-') << std::setw(3 * 25) << "" << std::setfill(' ') << std::endl;
 
-    mg_run_opts ro{version, threshold, max_phases, precision, 1};
+    mg_run_opts ro{version, threshold, max_phases, precision, 1, 0};
     mg_result *res = nullptr;
     st = mg_louvain_run(g, &ro, &res);
     if (st != MG_OK) {

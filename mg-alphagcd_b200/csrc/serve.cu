@@ -65,6 +65,7 @@ mg_run_opts default_run() {
     o.max_phases = 1000;
     o.precision = MG_PREC_FP64;
     o.verbose = 0;
+    o.keep_levels = 0;
     return o;
 }
 

@@ -4,6 +4,8 @@ Bar: bit-exact for bins, assignments, integral-weight coarsening and the
 modularity trace of integral graphs (both sides compute Q from exact integer
 sums); real weights within the tolerances written in each test.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -250,6 +252,12 @@ def test_mtx_loader_matches_oracle(O, ctx, tmp_path):
     off, cols, w = a.csr()
     assert (off == b.offsets).all() and (cols == b.cols).all() and (w == b.weights).all()
     assert a.louvain()["modularity"] == O.louvain(b)["modularity"]
+    # through the binary CSR cache (written, then mapped): the same graph
+    for flags in ({"cache_read": True, "cache_write": True}, {"cache_read": True}):
+        c = ctx.graph_from_mtx(str(gen), **flags)
+        off2, cols2, w2 = c.csr()
+        assert (off2 == off).all() and (cols2 == cols).all() and (w2 == w).all()
+    assert os.path.exists(str(gen) + ".mgcsr")
 
 
 def test_empty_and_edge_cases(O, ctx):
@@ -298,3 +306,22 @@ def test_unsorted_and_repeated_columns(O, ctx, duplicate):
         a = _up(ctx, g).louvain()
         b = O.louvain(g)
         _compare_runs(a, b)
+
+
+def test_dendrogram_levels_compose_to_assignment(O, ctx):
+    """keep_levels: one dense community map per level; composing them gives
+    the final assignment, which equals the oracle's."""
+    for g in (O.gen_sbm(65536, 64, 16.0, 0.8, seed=1), O.gen_rmat(14, seed=2)):
+        dg = _up(ctx, g)
+        a = dg.louvain(keep_levels=True)
+        maps = a["level_maps"]
+        assert len(maps) == a["levels"] == len(a["level_sizes"])
+        comp = np.arange(g.n, dtype=np.int64)
+        for lvl, m in enumerate(maps):
+            assert len(m) == a["level_sizes"][lvl]
+            nxt = a["level_sizes"][lvl + 1] if lvl + 1 < len(maps) else a["communities"]
+            assert m.max() + 1 == nxt and len(np.unique(m)) == nxt  # dense relabel
+            comp = m[comp]
+        assert (comp == a["assignment"]).all()
+        assert (a["assignment"] == O.louvain(g)["assignment"]).all()
+        assert "level_maps" not in dg.louvain()
