@@ -365,6 +365,14 @@ __device__ __forceinline__ typename ValT<WK>::type wget(const void *w, uint32_t 
     else return wload<WK>(w, e);
 }
 
+// an edge weight (double) as a table value: exact 32-bit integer for integral
+// weights (the f64 value plus 2^52 carries it in its low mantissa word)
+template <class V>
+__device__ __forceinline__ V wcast(double w) {
+    if constexpr (std::is_same<V, uint32_t>::value) return (uint32_t)__double2loint(__dadd_rn(w, 4503599627370496.0));
+    else return w;
+}
+
 template <class V>
 __device__ __forceinline__ double v2d(V v) {
     if constexpr (std::is_same<V, uint32_t>::value) return u2d(v);
@@ -446,6 +454,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
             const uint32_t base = wbase + lane;
             uint32_t jj[BATCH], cc[BATCH];
             V ww[BATCH];
+            // rows shorter than the batch: whole sub-steps past the row's end
+            // are skipped by the warp (uniform test)
 #pragma unroll
             for (int b = 0; b < BATCH; b++) {
                 uint32_t e = base + b * GT;
@@ -456,6 +466,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
             for (int b = 0; b < BATCH; b++) cc[b] = jj[b] != kEmpty ? vv.P[jj[b]] : kEmpty;
 #pragma unroll
             for (int b = 0; b < BATCH; b++) {
+                if (wbase + b * GT >= hi) break;
                 const uint32_t c = cc[b];
                 uint32_t hnew = kEmpty;  // slot this lane claimed for a new key
                 if (jj[b] != kEmpty) {
@@ -507,7 +518,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
         const uint32_t nd = cnt[par][g];
         G best = G(0);
         uint32_t dst = src;
-        for (uint32_t u0 = t; u0 < nd; u0 += GT * EB) {
+        for (uint32_t ub = t & ~31u; ub < nd; ub += GT * EB) {  // warp-uniform
+            const uint32_t u0 = ub + lane;
             uint32_t kk[EB];
             double sc[EB], kv[EB];
 #pragma unroll
@@ -589,8 +601,9 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
 // collects its sum (see the two fill modes below), each CTA evaluates the
 // candidates of its segment, and rank 0 reduces the CS winners through
 // distributed shared memory.  Two cluster barriers per
-// vertex (accumulators double-buffered).  Integral weights use packed 64-bit
-// slots {key:32 | sum:32}.
+// vertex (accumulators double-buffered).  Slots are a 32-bit key and a sum:
+// 32-bit integer for integral weights (shared-memory 32-bit adds; 64-bit
+// packed slots were slower under contention), else double.
 // ============================================================================
 namespace cg = cooperative_groups;
 constexpr int kClusterThreads = 1024;  // one CTA per SM with a 16K-slot segment
@@ -616,11 +629,12 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
     constexpr int BATCH = 4;
     constexpr int EB = 4;  // slots per thread per evaluation batch
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    uint64_t *packed = (uint64_t *)smem_raw;                 // integral weights
-    uint32_t *keys = (uint32_t *)smem_raw;                   // real weights
-    double *vals = (double *)(smem_raw + sizeof(uint32_t) * S);
+    // keys u32 [S] | sums [S] (u32 for integral weights, else double) | used u16 [S]
+    using CV = typename ValT<WK>::type;
+    uint32_t *keys = (uint32_t *)smem_raw;
+    CV *vals = (CV *)(smem_raw + sizeof(uint32_t) * S);
     // slots of this CTA's segment that received a new key, in insertion order
-    uint16_t *used = (uint16_t *)(smem_raw + (kIntg<WK> ? sizeof(uint64_t) : sizeof(uint32_t) + sizeof(double)) * S);
+    uint16_t *used = (uint16_t *)(smem_raw + (sizeof(uint32_t) + sizeof(CV)) * S);
     __shared__ uint32_t ucnt;
     __shared__ double acc_e[2], acc_s[2];
     __shared__ G best_g[2][CS];
@@ -630,11 +644,8 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
     unsigned rank = 0;
     if constexpr (CS > 1) rank = cg::this_cluster().block_rank();
     for (int s = threadIdx.x; s < S; s += kClusterThreads) {
-        if constexpr (kIntg<WK>) packed[s] = kEmpty64;
-        else {
-            keys[s] = kEmpty;
-            vals[s] = 0.0;
-        }
+        keys[s] = kEmpty;
+        vals[s] = CV(0);
     }
     if (threadIdx.x < 2) {
         acc_e[threadIdx.x] = 0;
@@ -681,6 +692,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
             for (int b = 0; b < BATCH; b++) cc[b] = jj[b] != kEmpty ? vv.P[jj[b]] : kEmpty;
 #pragma unroll
             for (int b = 0; b < BATCH; b++) {
+                if (wbase + b * step >= hi) break;  // uniform over the warp
                 const uint32_t c = cc[b];
                 uint32_t s = 0;
                 unsigned owner = 0;
@@ -695,77 +707,45 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
                     if (jj[b] != i) e_part += ww[b];
                     else s_part += ww[b];
                 }
+                CV wv = cand ? wcast<CV>(ww[b]) : CV(0);
                 if constexpr (kIntg<WK>) {
                     // lanes holding the same community add their weights in the
                     // warp; one leader per community inserts the sum (integer
                     // sums: the result does not depend on the grouping)
-                    uint32_t wsum = cand ? (uint32_t)ww[b] : 0u;
-                    bool lead = cand;
                     if (A.agg) {  // uniform: a kernel argument
                         const uint32_t peers = __match_any_sync(0xffffffffu, cand ? c : kEmpty);
-                        wsum = __reduce_add_sync(peers, wsum);
-                        lead = cand && (uint32_t)(__ffs(peers) - 1) == (threadIdx.x & 31u);
+                        wv = __reduce_add_sync(peers, wv);
+                        cand = cand && (uint32_t)(__ffs(peers) - 1) == (threadIdx.x & 31u);
                     }
-                    if (!lead) continue;
-                    const unsigned long long wi = wsum;
-                    uint64_t *seg = own ? packed : rank_ptr<CS>(packed, owner);
-                    uint16_t *useg = own ? used : rank_ptr<CS>(used, owner);
-                    uint32_t *uc = own ? &ucnt : rank_ptr<CS>(&ucnt, owner);
-                    bool placed = false;
-                    for (int p = 0; p < S; p++) {
-                        uint64_t cur = ((volatile uint64_t *)seg)[s];
-                        uint32_t k = (uint32_t)(cur >> 32);
-                        if (k == c) {
-                            atomicAdd((unsigned long long *)(seg + s), wi);
-                            placed = true;
-                            break;
-                        }
-                        if (k == kEmpty) {
-                            uint64_t prev = atomicCAS((unsigned long long *)(seg + s), kEmpty64, ((uint64_t)c << 32) | wi);
-                            if (prev == kEmpty64) {
-                                useg[atomicAdd(uc, 1u)] = (uint16_t)s;
-                                placed = true;
-                                break;
-                            }
-                            if ((uint32_t)(prev >> 32) == c) {
-                                atomicAdd((unsigned long long *)(seg + s), wi);
-                                placed = true;
-                                break;
-                            }
-                        }
-                        s = (s + 1) & (S - 1);
-                    }
-                    if (!placed) atomicAdd(&A.acc->overflow, 1ull);
-                } else {
-                    if (!cand) continue;
-                    uint32_t *ks = own ? keys : rank_ptr<CS>(keys, owner);
-                    double *vs = own ? vals : rank_ptr<CS>(vals, owner);
-                    uint16_t *useg = own ? used : rank_ptr<CS>(used, owner);
-                    uint32_t *uc = own ? &ucnt : rank_ptr<CS>(&ucnt, owner);
-                    bool placed = false;
-                    for (int p = 0; p < S; p++) {
-                        uint32_t cur = ((volatile uint32_t *)ks)[s];
-                        if (cur == c) {
-                            placed = true;
-                            break;
-                        }
-                        if (cur == kEmpty) {
-                            uint32_t prev = atomicCAS(ks + s, kEmpty, c);
-                            if (prev == kEmpty) {
-                                useg[atomicAdd(uc, 1u)] = (uint16_t)s;
-                                placed = true;
-                                break;
-                            }
-                            if (prev == c) {
-                                placed = true;
-                                break;
-                            }
-                        }
-                        s = (s + 1) & (S - 1);
-                    }
-                    if (placed) atomicAdd(vs + s, ww[b]);
-                    else atomicAdd(&A.acc->overflow, 1ull);
                 }
+                if (!cand) continue;
+                uint32_t *ks = own ? keys : rank_ptr<CS>(keys, owner);
+                CV *vs = own ? vals : rank_ptr<CS>(vals, owner);
+                uint16_t *useg = own ? used : rank_ptr<CS>(used, owner);
+                uint32_t *uc = own ? &ucnt : rank_ptr<CS>(&ucnt, owner);
+                bool placed = false;
+                for (int p = 0; p < S; p++) {
+                    uint32_t cur = ((volatile uint32_t *)ks)[s];
+                    if (cur == c) {
+                        placed = true;
+                        break;
+                    }
+                    if (cur == kEmpty) {
+                        uint32_t prev = atomicCAS(ks + s, kEmpty, c);
+                        if (prev == kEmpty) {
+                            useg[atomicAdd(uc, 1u)] = (uint16_t)s;
+                            placed = true;
+                            break;
+                        }
+                        if (prev == c) {
+                            placed = true;
+                            break;
+                        }
+                    }
+                    s = (s + 1) & (S - 1);
+                }
+                if (placed) atomicAdd(vs + s, wv);
+                else atomicAdd(&A.acc->overflow, 1ull);
             }
         }
         e_part = warp_sum(e_part);
@@ -779,7 +759,8 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
         G best = G(0);
         uint32_t dst = src;
         const uint32_t nd = ucnt;
-        for (uint32_t u0 = threadIdx.x; u0 < nd; u0 += kClusterThreads * EB) {
+        for (uint32_t ub = threadIdx.x & ~31u; ub < nd; ub += kClusterThreads * EB) {  // warp-uniform
+            const uint32_t u0 = ub + (threadIdx.x & 31u);
             uint32_t kk[EB];
             double kv[EB], sc[EB];
 #pragma unroll
@@ -788,17 +769,10 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
                 kk[b] = kEmpty;
                 if (u < nd) {
                     const uint32_t s = used[u];
-                    if constexpr (kIntg<WK>) {
-                        uint64_t v = packed[s];
-                        kk[b] = (uint32_t)(v >> 32);
-                        kv[b] = u2d((uint32_t)v);
-                        packed[s] = kEmpty64;
-                    } else {
-                        kk[b] = keys[s];
-                        kv[b] = vals[s];
-                        keys[s] = kEmpty;
-                        vals[s] = 0.0;
-                    }
+                    kk[b] = keys[s];
+                    kv[b] = v2d(vals[s]);
+                    keys[s] = kEmpty;
+                    vals[s] = CV(0);
                 }
             }
 #pragma unroll
@@ -1034,7 +1008,7 @@ __global__ void heavy_final_kernel(LMArgs A, const uint32_t *hv, uint32_t H, con
 
 template <int CS, int WK, int PREC, int VER, int BT>
 size_t cluster_smem() {
-    return (size_t)kClusterSlots * ((kIntg<WK> ? sizeof(uint64_t) : sizeof(uint32_t) + sizeof(double)) + sizeof(uint16_t));
+    return (size_t)kClusterSlots * (sizeof(uint32_t) + sizeof(typename ValT<WK>::type) + sizeof(uint16_t));
 }
 
 template <int CS, int WK, int PREC, int VER, int BT>
