@@ -191,13 +191,15 @@ def peaks():
 
 
 def traffic_per_sweep():
-    """DRAM bytes of one phase-0 sweep from the committed ncu summary, if any."""
+    """DRAM bytes of the first level-0 sweep from the committed ncu summary,
+    with the algorithmic bytes of that same sweep (or Nones)."""
     path = os.path.join(ROOT, "profiles", "local_move_rmat24_traffic.json")
     try:
         with open(path) as f:
-            return json.load(f).get("dram_bytes_per_sweep")
+            p = json.load(f)
+        return p.get("dram_bytes_per_sweep"), p.get("algorithmic_bytes_per_sweep")
     except (OSError, ValueError):
-        return None
+        return None, None
 
 
 def cpu_baseline_sample(csr, threads):
@@ -482,7 +484,7 @@ def run_engine(args, world, rank, local, pg):
     sweeps = sum(r["sweeps"] for r in runs)
     achieved = sweep_b / sweep_s / 1e9
     peak, peak_kind = peaks()
-    traffic = traffic_per_sweep()
+    traffic, traffic_alg = traffic_per_sweep()
 
     # end to end through the public API with host buffers: upload the CSR,
     # run, read the assignment back
@@ -545,6 +547,8 @@ def run_engine(args, world, rank, local, pg):
         "local_move_s": last["seconds_local_move"], "coarsen_s": last["seconds_coarsen"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
+                     "traffic_sweep": "first level-0 sweep (ncu, profiles/local_move_rmat24_traffic.md)",
+                     "traffic_sweep_algorithmic_bytes": traffic_alg,
                      "kernel": "local-move sweep (all bins)", "peak_kind": peak_kind,
                      "sweeps": sweeps, "algorithmic_bytes_per_sweep": sweep_b / max(sweeps, 1)},
         "cpu_baseline": cpu,
