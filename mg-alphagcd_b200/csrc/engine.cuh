@@ -120,6 +120,7 @@ constexpr uint32_t kTuneMinVertices = 4096;  // smaller classes keep the default
 
 struct MoveWorkspace {
     DBuf<uint32_t> perm;
+    DBuf<uint2> rows;              // {off[perm[q]], off[perm[q] + 1]} per class-list entry q
     int max_cluster = 0;           // largest cluster size the device runs (8 or 16)
     // heavy-vertex global tables
     DBuf<uint64_t> h_toff;         // table offset per heavy vertex (H+1)

@@ -25,6 +25,10 @@ struct LMArgs {
     const double *__restrict__ k;
     const double *__restrict__ sigma;
     const uint32_t *__restrict__ perm;
+    // single-graph sweeps: the row range of every class-list entry, read
+    // beside perm so that a vertex's edges do not wait for its id (NULL in
+    // batched sweeps)
+    const uint2 *__restrict__ rows;
     GainK K;             // gain constants of the graph
     int up;
     int integral;
@@ -220,11 +224,18 @@ __global__ void __launch_bounds__(256) lm_tile_kernel(LMArgs A, uint32_t bin_off
         VView vv;
         if (active) {
             i = A.perm[bin_off + idx];
+            if constexpr (BT == 0) {
+                const uint2 r = A.rows[bin_off + idx];
+                lo = r.x;
+                hi = r.y;
+            }
             active = vview_at<BT>(A, bin_off + idx, vv);
         }
         if (active) {
-            lo = A.off[i];
-            hi = A.off[i + 1];
+            if constexpr (BT != 0) {
+                lo = A.off[i];
+                hi = A.off[i + 1];
+            }
             src = vv.P[i];
         }
         const uint32_t e = lo + gl;
@@ -435,11 +446,18 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
         VView vv;
         if (active) {
             i = A.perm[bin_off + idx];
+            if constexpr (BT == 0) {
+                const uint2 r = A.rows[bin_off + idx];
+                lo = r.x;
+                hi = r.y;
+            }
             active = vview_at<BT>(A, bin_off + idx, vv);
         }
         if (active) {
-            lo = A.off[i];
-            hi = A.off[i + 1];
+            if constexpr (BT != 0) {
+                lo = A.off[i];
+                hi = A.off[i + 1];
+            }
             src = vv.P[i];
             ki = A.k[i];
             a = A.sigma[src] - ki;  // issued early, consumed after the edge pass

@@ -36,6 +36,14 @@ namespace {
 
 using namespace lmk;
 
+// row range of every class-list entry (class order)
+__global__ void row_ranges_kernel(const uint32_t *off, const uint32_t *perm, uint32_t n, uint2 *rows) {
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const uint32_t i = perm[q];
+        rows[q] = make_uint2(off[i], off[i + 1]);
+    }
+}
+
 __global__ void heavy_layout_kernel(const uint32_t *off, const uint32_t *hv, uint32_t H, uint32_t *tsize,
                                     uint32_t *ins_cnt, uint32_t *eval_cnt, uint64_t *tsz64) {
     uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
@@ -159,6 +167,12 @@ void move_prepare_level(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, c
     ws.acc.ensure(1);
     uint32_t *perm = ws.perm.ensure(g.n + 1);
     compute_bins(kSweepScheme, g.n, g.off, perm, lvl.bins, s, ws.prim);
+    uint2 *rows = ws.rows.ensure(g.n + 1);
+    if (g.n) {
+        row_ranges_kernel<<<(unsigned)std::min<uint64_t>(ceil_div(g.n, 256), 148 * 16), 256, 0, s>>>(g.off, perm, g.n,
+                                                                                                     rows);
+        MG_LAUNCH_CHECK();
+    }
     for (int c = 0; c < kLightClasses; c++) lvl.shape[c] = (uint8_t)default_shape(c);
     const uint32_t h0 = lvl.bins.offset[kFirstHeavyClass];
     lvl.heavy = g.n - h0;
@@ -237,6 +251,7 @@ LMArgs single_args(const GraphView &g, MoveWorkspace &ws, const SweepParams &p, 
     A.k = k;
     A.sigma = sigma;
     A.perm = ws.perm.get();
+    A.rows = ws.rows.get();
     A.K = gain_constants(p.mass);
     A.up = p.up;
     A.integral = p.integral;
