@@ -30,11 +30,15 @@ __global__ void apply_relabel_kernel(const uint32_t *C, uint32_t n, const uint32
 }
 
 // key = (C'[u] << bc) | C'[v] per edge (u,v), payload = weight (if any).
-// Edge-parallel: a warp takes 512 consecutive edges (lane-strided, coalesced),
-// finds the row of the first by binary search and walks rows forward.
+// Row walk: a warp takes 512 consecutive edges (lane-strided, coalesced),
+// finds the row of the first by binary search and every lane walks rows
+// forward.  Measured faster than the tiled kernel below on unit-weight levels
+// (R-MAT-24 level 0: 41 vs 43 ms) and on the levels of a batched union (the
+// 4,096-SBM batch: 0.33 vs 0.38 s of coarsening), slower on weighted
+// single-graph levels (R-MAT-24 level 1: 69 vs 55 ms of coarsening).
 template <int WK>
-__global__ void expand_keys_kernel(const uint32_t *off, const uint32_t *col, const void *w, uint32_t n, uint64_t m,
-                                   const uint32_t *Cd, int bc, uint64_t *keys, double *vals) {
+__global__ void expand_keys_walk_kernel(const uint32_t *off, const uint32_t *col, const void *w, uint32_t n,
+                                        uint64_t m, const uint32_t *Cd, int bc, uint64_t *keys, double *vals) {
     constexpr int PER = 16;
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -66,6 +70,113 @@ __global__ void expand_keys_kernel(const uint32_t *off, const uint32_t *col, con
             if constexpr (WK == WK_F32) vals[e] = (double)((const float *)w)[e];
             else if constexpr (WK == WK_F64) vals[e] = ((const double *)w)[e];
         }
+    }
+}
+
+// Tiled: a block takes a tile of kExpandTile consecutive edges.  The rows that start
+// inside the tile are marked at their first edge (a row id per position; of
+// several rows starting at one position -- empty rows -- the largest, which is
+// the non-empty one, wins), a prefix maximum over the tile then gives every
+// edge its row, and the keys are written with coalesced loads and stores.
+// One binary search per tile finds the row holding its first edge.
+constexpr int kExpandThreads = 256;
+constexpr int kExpandPer = 16;
+constexpr uint32_t kExpandTile = kExpandThreads * kExpandPer;
+
+template <int WK>
+__global__ void __launch_bounds__(kExpandThreads) expand_keys_kernel(const uint32_t *off, const uint32_t *col,
+                                                                     const void *w, uint32_t n, uint64_t m,
+                                                                     const uint32_t *Cd, int bc, uint64_t *keys,
+                                                                     double *vals) {
+    // tile position q lives at q + q/32 (one padding word per 32: the
+    // per-thread runs of 16 positions then fall on distinct banks)
+    __shared__ uint32_t rowat[kExpandTile + kExpandTile / 32];
+    __shared__ uint32_t part[kExpandThreads];
+    __shared__ uint32_t r0s;
+    const uint32_t t = threadIdx.x;
+    for (uint64_t E0 = (uint64_t)blockIdx.x * kExpandTile; E0 < m; E0 += (uint64_t)gridDim.x * kExpandTile) {
+        const uint64_t E1 = E0 + kExpandTile < m ? E0 + kExpandTile : m;
+        if (t == 0) {
+            uint32_t lo = 0, hi = n - 1;  // last row with off[row] <= E0: the row of edge E0
+            while (lo < hi) {
+                const uint32_t mid = lo + ((hi - lo + 1) >> 1);
+                if (off[mid] <= E0) lo = mid;
+                else hi = mid - 1;
+            }
+            r0s = lo;
+        }
+        for (uint32_t q = t; q < kExpandTile + kExpandTile / 32; q += kExpandThreads) rowat[q] = 0;
+        __syncthreads();
+        const uint32_t r0 = r0s;
+        if (t == 0) rowat[0] = r0;
+        // rows r0+1, r0+2, ... that start inside the tile, 256 at a time
+        for (uint32_t base = r0 + 1;; base += kExpandThreads) {
+            const uint32_t j = base + t;
+            bool inside = false;
+            if (j < n) {
+                const uint32_t st = off[j];
+                inside = st < E1;
+                if (inside) {
+                    const uint32_t q = (uint32_t)(st - E0);
+                    atomicMax(&rowat[q + (q >> 5)], j);
+                }
+            }
+            // offsets are monotone: more rows can start inside only if the
+            // batch's last one did
+            if (!__syncthreads_or(t == kExpandThreads - 1 && inside)) break;
+        }
+        __syncthreads();
+        // prefix maximum: 16 positions per thread, then across the threads
+        uint32_t run = 0;
+#pragma unroll
+        for (int k = 0; k < kExpandPer; k++) {
+            const uint32_t q = t * kExpandPer + k;
+            run = max(run, rowat[q + (q >> 5)]);
+            rowat[q + (q >> 5)] = run;
+        }
+        part[t] = run;
+        __syncthreads();
+        if (t < 32) {
+            // exclusive prefix maximum of the 256 thread maxima: 8 per lane
+            constexpr int L = kExpandThreads / 32;
+            uint32_t loc[L], v = 0;
+#pragma unroll
+            for (int k = 0; k < L; k++) {
+                v = max(v, part[t * L + k]);
+                loc[k] = v;
+            }
+            uint32_t inc = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+                if ((int)t >= o) inc = max(inc, y);
+            }
+            uint32_t ex = __shfl_up_sync(0xffffffffu, inc, 1);
+            if (t == 0) ex = 0;
+#pragma unroll
+            for (int k = 0; k < L; k++) part[t * L + k] = k ? max(ex, loc[k - 1]) : ex;
+        }
+        __syncthreads();
+        {
+            const uint32_t pre = part[t];
+#pragma unroll
+            for (int k = 0; k < kExpandPer; k++) {
+                const uint32_t q = t * kExpandPer + k;
+                rowat[q + (q >> 5)] = max(rowat[q + (q >> 5)], pre);
+            }
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int k = 0; k < kExpandPer; k++) {
+            const uint32_t q = k * kExpandThreads + t;
+            const uint64_t e = E0 + q;
+            if (e < E1) {
+                keys[e] = ((uint64_t)Cd[rowat[q + (q >> 5)]] << bc) | Cd[__ldcs(col + e)];
+                if constexpr (WK == WK_F32) vals[e] = (double)__ldcs((const float *)w + e);
+                else if constexpr (WK == WK_F64) vals[e] = __ldcs((const double *)w + e);
+            }
+        }
+        __syncthreads();  // rowat is reused by the next tile
     }
 }
 
@@ -254,7 +365,7 @@ uint32_t relabel_dense(const uint32_t *C, uint32_t n, uint32_t *C_dense, Coarsen
 }
 
 void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int integral, LevelGraph &out,
-                   CoarsenWorkspace &ws, cudaStream_t s, uint64_t *upper_degree_off) {
+                   CoarsenWorkspace &ws, cudaStream_t s, uint64_t *upper_degree_off, bool tiled_expand) {
     const size_t m = g.nnz;
     const int bc = bits_for(n_new);
     if (upper_degree_off) {
@@ -276,11 +387,19 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
     const bool weighted = g.wk != WK_UNIT;
     double *vals = weighted ? ws.vals.ensure(m + 1) : nullptr;
     double *vals2 = weighted ? ws.vals_alt.ensure(m + 1) : nullptr;
-    unsigned gw = grid_for(ceil_div(m, 16), 256, 148ull * 64);
-    if (g.wk == WK_UNIT) expand_keys_kernel<WK_UNIT><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, vals);
-    else if (g.wk == WK_F32)
-        expand_keys_kernel<WK_F32><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, vals);
-    else expand_keys_kernel<WK_F64><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, vals);
+    if (g.wk == WK_UNIT || !tiled_expand) {
+        const unsigned gw = grid_for(ceil_div(m, 16), 256, 148ull * 64);
+        if (g.wk == WK_UNIT)
+            expand_keys_walk_kernel<WK_UNIT><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, vals);
+        else if (g.wk == WK_F32)
+            expand_keys_walk_kernel<WK_F32><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, vals);
+        else expand_keys_walk_kernel<WK_F64><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, vals);
+    } else {
+        const unsigned gw = grid_for(ceil_div(m, kExpandTile), kExpandThreads, 148ull * 8);
+        if (g.wk == WK_F32)
+            expand_keys_kernel<WK_F32><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, vals);
+        else expand_keys_kernel<WK_F64><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, vals);
+    }
     MG_LAUNCH_CHECK();
     bool flipped;
     if (weighted) flipped = radix_sort<double>(keys, vals, keys2, vals2, m, 2 * bc, s, ws.prim);
