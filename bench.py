@@ -211,6 +211,13 @@ def cpu_baseline_sample(csr, threads):
     return edges / t, t
 
 
+def rmat_config(scale, n, nnz, parallelism):
+    """The workload description both arms report."""
+    return {"workload": f"rmat{scale}_ef16_louvain_full", "vertices": n, "directed_entries": nnz,
+            "abcd": [RMAT["a"], RMAT["b"], RMAT["c"], 0.05], "seed": RMAT["seed"],
+            "l2": "inputs larger than L2 (2.1 GB of column ids)", "parallelism": parallelism}
+
+
 def run_reference(args, world, rank, local, pg):
     if rank != 0:
         return None
@@ -235,8 +242,7 @@ def run_reference(args, world, rank, local, pg):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded R-MAT generator)",
-        "config": {"workload": f"rmat{args.scale}_ef16_louvain", "vertices": g.n, "directed_entries": g.nnz,
-                   "parallelism": "host threads"},
+        "config": rmat_config(args.scale, g.n, g.nnz, f"host threads ({threads})"),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -536,10 +542,7 @@ def run_engine(args, world, rank, local, pg):
         "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded R-MAT generator, graph built on the device)",
-        "config": {"workload": f"rmat{args.scale}_ef16_louvain_full", "vertices": info["n"],
-                   "directed_entries": info["nnz"], "abcd": [RMAT["a"], RMAT["b"], RMAT["c"], 0.05],
-                   "seed": RMAT["seed"], "l2": "inputs larger than L2 (2.1 GB of column ids)",
-                   "parallelism": "replicas" if world > 1 else "single GPU"},
+        "config": rmat_config(args.scale, info["n"], info["nnz"], "replicas" if world > 1 else "single GPU"),
         "modularity": last["modularity"], "communities": last["communities"],
         "levels": [int(x) for x in last["level_sizes"]], "iterations": last["iterations"],
         "first_pass_edges_per_s": last["phase0_edges_swept"] / last["phase0_seconds"],
