@@ -5,9 +5,10 @@
 // to batch, so a warm worker allocates and frees no device memory (cudaFree
 // would wait for the whole device and stall the other workers).  A free
 // worker takes the queued jobs in arrival order -- the head job and the ones
-// behind it with the same kind of input and run options -- until its share of
-// the HBM budget (budget / slots, by a per-job upper-bound estimate) or the
-// job cap is reached, and runs them as one batch; the workers' batches run on
+// behind it with the same kind of input and run options and a similar size
+// (within 8x of the head job's memory estimate) -- until its share of the HBM
+// budget (budget / slots, by a per-job upper-bound estimate) or the job cap is
+// reached, and runs them as one batch; the workers' batches run on
 // their own streams and overlap on the GPU.  A job is complete as soon as its
 // own graph finishes inside the batch (batch_run's per-graph callback), not
 // when the whole batch ends.
@@ -52,6 +53,9 @@ struct Job {
 // active lists, bins), per directed entry the union CSR, the generator's pairs
 // and sort keys, and the coarsening keys of the first level.
 size_t estimate_bytes(uint64_t n, uint64_t nnz) { return 160 * n + 64 * nnz + (1ull << 20); }
+
+// largest size ratio (device-memory estimate) between two jobs of one batch
+constexpr size_t kBatchSizeRatio = 8;
 
 bool same_run(const mg_run_opts &a, const mg_run_opts &b) {
     return a.version == b.version && a.threshold == b.threshold && a.max_phases == b.max_phases &&
@@ -207,6 +211,12 @@ void worker_main(mg_server *S) {
             while (!S->queue.empty() && take.size() < S->opts.max_batch_jobs) {
                 Job *j = S->queue.front();
                 if (j->csr != head->csr || !same_run(j->opts, head->opts) || used + j->bytes > S->share) break;
+                // jobs of similar size only: a batch holds its slot until its
+                // slowest graph is done, so a large job among small ones would
+                // keep the slot (and its memory share) long after they finished
+                if (!take.empty() && (j->bytes > kBatchSizeRatio * head->bytes ||
+                                      head->bytes > kBatchSizeRatio * j->bytes))
+                    break;
                 used += j->bytes;
                 take.push_back(j);
                 S->queue.pop_front();
