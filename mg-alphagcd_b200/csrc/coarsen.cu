@@ -14,6 +14,7 @@
 // community.  For integral weights the merged sums are exact (prefix sums
 // over 64-bit integers); for real weights they are double sums.
 #include <algorithm>
+#include <type_traits>
 
 #include "engine.cuh"
 
@@ -36,9 +37,9 @@ __global__ void apply_relabel_kernel(const uint32_t *C, uint32_t n, const uint32
 // (R-MAT-24 level 0: 41 vs 43 ms) and on the levels of a batched union (the
 // 4,096-SBM batch: 0.33 vs 0.38 s of coarsening), slower on weighted
 // single-graph levels (R-MAT-24 level 1: 69 vs 55 ms of coarsening).
-template <int WK>
+template <int WK, class PV>
 __global__ void expand_keys_walk_kernel(const uint32_t *off, const uint32_t *col, const void *w, uint32_t n,
-                                        uint64_t m, const uint32_t *Cd, int bc, uint64_t *keys, double *vals) {
+                                        uint64_t m, const uint32_t *Cd, int bc, uint64_t *keys, PV *vals) {
     constexpr int PER = 16;
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -67,8 +68,8 @@ __global__ void expand_keys_walk_kernel(const uint32_t *off, const uint32_t *col
                 kr = (uint64_t)Cd[r] << bc;
             }
             keys[e] = kr | Cd[__ldcs(col + e)];
-            if constexpr (WK == WK_F32) vals[e] = (double)((const float *)w)[e];
-            else if constexpr (WK == WK_F64) vals[e] = ((const double *)w)[e];
+            if constexpr (WK == WK_F32) vals[e] = (PV)((const float *)w)[e];
+            else if constexpr (WK == WK_F64) vals[e] = (PV)((const double *)w)[e];
         }
     }
 }
@@ -83,11 +84,11 @@ constexpr int kExpandThreads = 256;
 constexpr int kExpandPer = 16;
 constexpr uint32_t kExpandTile = kExpandThreads * kExpandPer;
 
-template <int WK>
+template <int WK, class PV>
 __global__ void __launch_bounds__(kExpandThreads) expand_keys_kernel(const uint32_t *off, const uint32_t *col,
                                                                      const void *w, uint32_t n, uint64_t m,
                                                                      const uint32_t *Cd, int bc, uint64_t *keys,
-                                                                     double *vals) {
+                                                                     PV *vals) {
     // tile position q lives at q + q/32 (one padding word per 32: the
     // per-thread runs of 16 positions then fall on distinct banks)
     __shared__ uint32_t rowat[kExpandTile + kExpandTile / 32];
@@ -172,8 +173,8 @@ __global__ void __launch_bounds__(kExpandThreads) expand_keys_kernel(const uint3
             const uint64_t e = E0 + q;
             if (e < E1) {
                 keys[e] = ((uint64_t)Cd[rowat[q + (q >> 5)]] << bc) | Cd[__ldcs(col + e)];
-                if constexpr (WK == WK_F32) vals[e] = (double)__ldcs((const float *)w + e);
-                else if constexpr (WK == WK_F64) vals[e] = __ldcs((const double *)w + e);
+                if constexpr (WK == WK_F32) vals[e] = (PV)__ldcs((const float *)w + e);
+                else if constexpr (WK == WK_F64) vals[e] = (PV)__ldcs((const double *)w + e);
             }
         }
         __syncthreads();  // rowat is reused by the next tile
@@ -229,7 +230,8 @@ __global__ void run_lengths_kernel(const uint32_t *ustart, uint32_t u, uint32_t 
 }
 
 // integral weights: exact prefix sums over uint64, run sum = prefix difference
-__global__ void to_u64_kernel(const double *v, size_t m, uint64_t *o) {
+template <class T>
+__global__ void to_u64_kernel(const T *v, size_t m, uint64_t *o) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x)
         o[i] = (uint64_t)v[i];
 }
@@ -387,22 +389,35 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
     const bool weighted = g.wk != WK_UNIT;
     double *vals = weighted ? ws.vals.ensure(m + 1) : nullptr;
     double *vals2 = weighted ? ws.vals_alt.ensure(m + 1) : nullptr;
-    if (g.wk == WK_UNIT || !tiled_expand) {
-        const unsigned gw = grid_for(ceil_div(m, 16), 256, 148ull * 64);
-        if (g.wk == WK_UNIT)
-            expand_keys_walk_kernel<WK_UNIT><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, vals);
-        else if (g.wk == WK_F32)
-            expand_keys_walk_kernel<WK_F32><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, vals);
-        else expand_keys_walk_kernel<WK_F64><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, vals);
-    } else {
-        const unsigned gw = grid_for(ceil_div(m, kExpandTile), kExpandThreads, 148ull * 8);
-        if (g.wk == WK_F32)
-            expand_keys_kernel<WK_F32><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, vals);
-        else expand_keys_kernel<WK_F64><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, vals);
-    }
-    MG_LAUNCH_CHECK();
+    // integral weights travel through the sort as 32-bit integers (exact:
+    // every weight of an integral graph is below 2^32), real ones as double
+    const bool ipay = weighted && integral;
+    uint32_t *ivals = (uint32_t *)vals, *ivals2 = (uint32_t *)vals2;
+    auto expand = [&](auto *pv) {
+        using PV = typename std::remove_pointer<decltype(pv)>::type;
+        if (g.wk == WK_UNIT || !tiled_expand) {
+            const unsigned gw = grid_for(ceil_div(m, 16), 256, 148ull * 64);
+            if (g.wk == WK_UNIT)
+                expand_keys_walk_kernel<WK_UNIT, PV><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
+            else if (g.wk == WK_F32)
+                expand_keys_walk_kernel<WK_F32, PV><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
+            else expand_keys_walk_kernel<WK_F64, PV><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
+        } else {
+            const unsigned gw = grid_for(ceil_div(m, kExpandTile), kExpandThreads, 148ull * 8);
+            if (g.wk == WK_F32)
+                expand_keys_kernel<WK_F32, PV><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys,
+                                                                             pv);
+            else
+                expand_keys_kernel<WK_F64, PV><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys,
+                                                                             pv);
+        }
+        MG_LAUNCH_CHECK();
+    };
+    if (ipay) expand(ivals);
+    else expand(vals);
     bool flipped;
-    if (weighted) flipped = radix_sort<double>(keys, vals, keys2, vals2, m, 2 * bc, s, ws.prim);
+    if (ipay) flipped = radix_sort<uint32_t>(keys, ivals, keys2, ivals2, m, 2 * bc, s, ws.prim);
+    else if (weighted) flipped = radix_sort<double>(keys, vals, keys2, vals2, m, 2 * bc, s, ws.prim);
     else flipped = radix_sort<NoVal>(keys, (NoVal *)nullptr, keys2, (NoVal *)nullptr, m, 2 * bc, s, ws.prim);
     const uint64_t *sk = flipped ? keys2 : keys;
     const double *sv = flipped ? vals2 : vals;
@@ -415,7 +430,7 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
     } else if (integral) {
         // exact: 64-bit prefix sums over the sorted weights, run sum = difference
         uint64_t *pre = (uint64_t *)(flipped ? vals : vals2);
-        to_u64_kernel<<<grid_for(m), 256, 0, s>>>(sv, m, pre);
+        to_u64_kernel<uint32_t><<<grid_for(m), 256, 0, s>>>(flipped ? ivals2 : ivals, m, pre);
         MG_LAUNCH_CHECK();
         exclusive_scan<uint64_t>(pre, pre, m, pre + m, s, ws.prim);
         run_diff_kernel<<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)m, pre, w);
