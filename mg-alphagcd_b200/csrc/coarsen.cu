@@ -403,7 +403,8 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
                 expand_keys_walk_kernel<WK_F32, PV><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
             else expand_keys_walk_kernel<WK_F64, PV><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
         } else {
-            const unsigned gw = grid_for(ceil_div(m, kExpandTile), kExpandThreads, 148ull * 8);
+            // one block per tile, at most 8 resident per SM (grid-stride over tiles)
+            const unsigned gw = grid_for(ceil_div(m, kExpandTile), 1, 148ull * 8);
             if (g.wk == WK_F32)
                 expand_keys_kernel<WK_F32, PV><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys,
                                                                              pv);
