@@ -31,50 +31,7 @@ __global__ void apply_relabel_kernel(const uint32_t *C, uint32_t n, const uint32
 }
 
 // key = (C'[u] << bc) | C'[v] per edge (u,v), payload = weight (if any).
-// Row walk: a warp takes 512 consecutive edges (lane-strided, coalesced),
-// finds the row of the first by binary search and every lane walks rows
-// forward.  Measured faster than the tiled kernel below on unit-weight levels
-// (R-MAT-24 level 0: 41 vs 43 ms) and on the levels of a batched union (the
-// 4,096-SBM batch: 0.33 vs 0.38 s of coarsening), slower on weighted
-// single-graph levels (R-MAT-24 level 1: 69 vs 55 ms of coarsening).
-template <int WK, class PV>
-__global__ void expand_keys_walk_kernel(const uint32_t *off, const uint32_t *col, const void *w, uint32_t n,
-                                        uint64_t m, const uint32_t *Cd, int bc, uint64_t *keys, PV *vals) {
-    constexpr int PER = 16;
-    const uint32_t lane = threadIdx.x & 31;
-    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t t0 = warp * 32 * PER; t0 < m; t0 += nw * 32 * PER) {
-        uint32_t r = 0;
-        if (lane == 0) {
-            uint32_t lo = 0, hi = n - 1;  // last row with off[row] <= t0
-            while (lo < hi) {
-                uint32_t mid = lo + ((hi - lo + 1) >> 1);
-                if (off[mid] <= t0) lo = mid;
-                else hi = mid - 1;
-            }
-            r = lo;
-        }
-        r = __shfl_sync(0xffffffffu, r, 0);
-        uint32_t cr = kEmpty;
-        uint64_t kr = 0;
-#pragma unroll 4
-        for (int k = 0; k < PER; k++) {
-            const uint64_t e = t0 + (uint64_t)k * 32 + lane;
-            if (e >= m) break;
-            while (off[r + 1] <= e) r++;
-            if (r != cr) {
-                cr = r;
-                kr = (uint64_t)Cd[r] << bc;
-            }
-            keys[e] = kr | Cd[__ldcs(col + e)];
-            if constexpr (WK == WK_F32) vals[e] = (PV)((const float *)w)[e];
-            else if constexpr (WK == WK_F64) vals[e] = (PV)((const double *)w)[e];
-        }
-    }
-}
-
-// Tiled: a block takes a tile of kExpandTile consecutive edges.  The rows that start
+// A block takes a tile of kExpandTile consecutive edges.  The rows that start
 // inside the tile are marked at their first edge (a row id per position; of
 // several rows starting at one position -- empty rows -- the largest, which is
 // the non-empty one, wins), a prefix maximum over the tile then gives every
@@ -367,7 +324,7 @@ uint32_t relabel_dense(const uint32_t *C, uint32_t n, uint32_t *C_dense, Coarsen
 }
 
 void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int integral, LevelGraph &out,
-                   CoarsenWorkspace &ws, cudaStream_t s, uint64_t *upper_degree_off, bool tiled_expand) {
+                   CoarsenWorkspace &ws, cudaStream_t s, uint64_t *upper_degree_off) {
     const size_t m = g.nnz;
     const int bc = bits_for(n_new);
     if (upper_degree_off) {
@@ -393,25 +350,15 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
     // every weight of an integral graph is below 2^32), real ones as double
     const bool ipay = weighted && integral;
     uint32_t *ivals = (uint32_t *)vals, *ivals2 = (uint32_t *)vals2;
+    // one block per tile, at most 8 resident per SM (grid-stride over tiles)
+    const unsigned gw = grid_for(ceil_div(m, kExpandTile), 1, 148ull * 8);
     auto expand = [&](auto *pv) {
         using PV = typename std::remove_pointer<decltype(pv)>::type;
-        if (g.wk == WK_UNIT || !tiled_expand) {
-            const unsigned gw = grid_for(ceil_div(m, 16), 256, 148ull * 64);
-            if (g.wk == WK_UNIT)
-                expand_keys_walk_kernel<WK_UNIT, PV><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
-            else if (g.wk == WK_F32)
-                expand_keys_walk_kernel<WK_F32, PV><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
-            else expand_keys_walk_kernel<WK_F64, PV><<<gw, 256, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
-        } else {
-            // one block per tile, at most 8 resident per SM (grid-stride over tiles)
-            const unsigned gw = grid_for(ceil_div(m, kExpandTile), 1, 148ull * 8);
-            if (g.wk == WK_F32)
-                expand_keys_kernel<WK_F32, PV><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys,
-                                                                             pv);
-            else
-                expand_keys_kernel<WK_F64, PV><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys,
-                                                                             pv);
-        }
+        if (g.wk == WK_UNIT)
+            expand_keys_kernel<WK_UNIT, PV><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
+        else if (g.wk == WK_F32)
+            expand_keys_kernel<WK_F32, PV><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
+        else expand_keys_kernel<WK_F64, PV><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
         MG_LAUNCH_CHECK();
     };
     if (ipay) expand(ivals);

@@ -257,11 +257,8 @@ struct LevelGraph {
 // Dense order-preserving relabel; returns n'.
 uint32_t relabel_dense(const uint32_t *C, uint32_t n, uint32_t *C_dense, CoarsenWorkspace &ws, cudaStream_t s);
 // Next level from a graph and a dense assignment with n' communities.
-// tiled_expand: build the sort keys of weighted levels with the tiled kernel
-// (single graphs) rather than the row walk (batched unions); same keys.
 void coarsen_level(const GraphView &g, const uint32_t *C_dense, uint32_t n_new, int integral, LevelGraph &out,
-                   CoarsenWorkspace &ws, cudaStream_t s, uint64_t *upper_degree_off /* device, may be null */,
-                   bool tiled_expand = true);
+                   CoarsenWorkspace &ws, cudaStream_t s, uint64_t *upper_degree_off /* device, may be null */);
 
 // Build a symmetric deduplicated CSR from undirected pairs already on the
 // device (self-loops dropped); used by the generators.  With pair weights w
