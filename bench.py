@@ -341,16 +341,20 @@ def run_loader(mg, ctx, scale=20):
         parse = min(timed(0) for _ in range(3))
         write = timed(mg.LOAD_CACHE_WRITE)
         cached = min(timed(mg.LOAD_CACHE_READ) for _ in range(3))
-        t0 = time.perf_counter()
-        h = ctx.graph_from_mtx(path, cache_read=True)
-        up = time.perf_counter() - t0
-        same = bool((h.csr()[1] == cols).all())
-        h.close()
+        ups, same = [], False
+        for rep in range(3):  # the first call also pays device allocations and page faults
+            t0 = time.perf_counter()
+            h = ctx.graph_from_mtx(path, cache_read=True)
+            ups.append(time.perf_counter() - t0)
+            if rep == 0:
+                same = bool((h.csr()[1] == cols).all())
+            h.close()
         return {"workload": f"R-MAT-{scale} (edge factor 16) as a symmetric pattern .mtx, {size / 1e6:.0f} MB, "
                             f"{len(cols)} directed entries", "threads": os.cpu_count(),
                 "parse_s": parse, "parse_mb_per_s": size / 1e6 / parse, "parse_entries_per_s": len(cols) / parse,
                 "parse_and_cache_write_s": write, "cache_load_s": cached,
-                "graph_from_cache_s": up, "graph_equals_generator": same}
+                "graph_from_cache_s": min(ups), "graph_from_cache_first_s": ups[0],
+                "graph_equals_generator": same}
     finally:
         shutil.rmtree(d, ignore_errors=True)
 
