@@ -458,9 +458,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
                 lo = A.off[i];
                 hi = A.off[i + 1];
             }
-            src = vv.P[i];
+            src = vv.P[i];  // needed first by the edge pass's community tests
             ki = A.k[i];
-            a = A.sigma[src] - ki;  // issued early, consumed after the edge pass
         }
         const int tb = table_bits(hi - lo, slots_log2);
         const uint32_t mask = (1u << tb) - 1u;
@@ -532,6 +531,10 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
             if (s_part != V(0)) atomicAdd(&acc_s[par][g], s_part);
         }
         group_sync<GT>();
+        // sigma of the vertex's own community: loaded here, beside the
+        // candidates' sigma, so that the edge loads above need not wait for
+        // the vertex's community id
+        if (active) a = A.sigma[src] - ki;
         const double e_src = v2d(acc_e[par][g]), selfw = v2d(acc_s[par][g]);
         const uint32_t nd = cnt[par][g];
         G best = G(0);
