@@ -685,7 +685,6 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
         if (!vview<BT>(A, i, vv)) continue;
         const uint32_t lo = A.off[i], hi = A.off[i + 1], src = vv.P[i];
         const double ki = A.k[i];
-        const double a = A.sigma[src] - ki;
         double e_part = 0, s_part = 0;
         // Two ways to fill the cluster's table, chosen per sweep:
         //  * distinct-heavy sweeps (no combining): every CTA reads the whole row
@@ -776,6 +775,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
             if (s_part != 0) atomicAdd(rank_ptr<CS>(&acc_s[par], 0), s_part);
         }
         cluster_barrier<CS>();  // all inserts and partial sums are in
+        const double a = A.sigma[src] - ki;  // loaded after the edge pass, beside the candidates' sigma
         const double e_src = *rank_ptr<CS>(&acc_e[par], 0);
         G best = G(0);
         uint32_t dst = src;
