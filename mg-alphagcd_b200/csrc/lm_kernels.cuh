@@ -6,6 +6,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <set>
 #include <utility>
@@ -1048,11 +1049,19 @@ cudaLaunchConfig_t cluster_config(size_t smem, unsigned grid, cudaStream_t s, cu
     return cfg;
 }
 
-// Maximum co-resident clusters of a cluster kernel (0 when the shape cannot run).
+// Maximum co-resident clusters of a cluster kernel (0 when the shape cannot
+// run) on the current device.  The first call per device also raises the
+// kernel's shared-memory limit there (a per-device setting); the result is
+// cached per device, under a lock, since serving workers launch concurrently.
 template <int CS, int WK, int PREC, int VER, int BT>
 int cluster_capacity() {
-    static int cap = -1;
-    if (cap >= 0) return cap;
+    static std::mutex mu;
+    static std::map<int, int> caps;  // device -> co-resident clusters
+    int dev = 0;
+    MG_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    const auto it = caps.find(dev);
+    if (it != caps.end()) return it->second;
     auto kern = lm_cluster_kernel<CS, WK, PREC, VER, BT>;
     const size_t smem = cluster_smem<CS, WK, PREC, VER, BT>();
     MG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1064,8 +1073,8 @@ int cluster_capacity() {
         cudaGetLastError();
         n = 0;
     }
-    cap = n;
-    return cap;
+    caps[dev] = n;
+    return n;
 }
 
 template <int CS, int WK, int PREC, int VER, int BT>
