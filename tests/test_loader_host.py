@@ -128,3 +128,17 @@ def test_malformed_files(mg, tmp_path):
     with pytest.raises(mg.MGError) as e:
         mg.load_mtx(str(tmp_path / "missing.mtx"))
     assert e.value.status == 4  # MG_ERR_IO
+
+
+def test_crlf_and_blank_padding_match_oracle(O, mg, tmp_path):
+    """Windows line ends and spaces before the first field: the same entries as
+    the oracle's atoi/atof reading.  A leading space is the "first space" of
+    the reference's field rule, so " 3 1 2.25" reads as row 3, column 3 (a
+    diagonal entry, dropped on the general path), as the reference does."""
+    text = ("%%MatrixMarket matrix coordinate real general\r\n% c\r\n6 6 6\r\n"
+            "2 1 0.5\r\n 3 1 2.25\r\n4 2 1\r\n  5 4 3\r\n6 5\r\n6 1 7.5\r\n")
+    p = tmp_path / "crlf.mtx"
+    p.write_bytes(text.encode())
+    a = mg.load_mtx(str(p))
+    _same(a, O.load_mtx(str(p)))
+    assert a["weights"].sum() == 2 * (0.5 + 1 + 1 + 7.5)
