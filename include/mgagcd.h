@@ -199,7 +199,8 @@ typedef struct {
     int max_phases;    /* default 1000 (src/main.cu:23) */
     int precision;     /* MG_PREC_* */
     int verbose;       /* print the reference's per-phase tables */
-    int keep_levels;   /* keep the dendrogram: every level's community map (mg_result_level_map) */
+    int keep_levels;   /* 1: keep the dendrogram, every level's community map (mg_result_level_map);
+                          2: also every level's graph on the host (mg_result_level_csr) */
 } mg_run_opts;
 
 typedef struct {
@@ -237,6 +238,15 @@ mg_status mg_result_level_sizes(const mg_result *r, uint32_t *out, int max, int 
  * (may be NULL) receives min(size, max) entries.  MG_ERR_INVALID when the
  * run did not keep levels or `level` is out of range. */
 mg_status mg_result_level_map(const mg_result *r, int level, uint32_t *out, uint32_t max, uint32_t *size);
+/* The graph level `level` worked on, for a run with keep_levels = 2 (level 0
+ * = the input graph, level l = the coarsened graph of phase l - 1, rows
+ * sorted by neighbour community): n, nnz and, for non-NULL pointers,
+ * offsets[n+1], cols[nnz], weights[nnz] (double; 1 for unit weights).  The
+ * reference coarsens its GpuGraph in place and keeps no level
+ * (src/coarsen_graph/coarsen_graph_mg.cu:2224-2228).  MG_ERR_INVALID when
+ * the run did not keep level graphs or `level` is out of range. */
+mg_status mg_result_level_csr(const mg_result *r, int level, uint32_t *n, uint64_t *nnz, uint64_t *offsets,
+                              uint32_t *cols, double *weights);
 /* the reference's printed table as rows {phase, loop, Q, dQ} */
 mg_status mg_result_trace(const mg_result *r, double *rows4, int max_rows, int *count);
 mg_status mg_result_destroy(mg_result *r);

@@ -116,7 +116,7 @@ EXPORTED = [
     "mg_serve_cancel", "mg_serve_release", "mg_serve_stats", "mg_serve_last_error", "mg_serve_stop",
     "mg_tune_mode", "mg_tune_table", "mg_tune_save", "mg_tune_load", "mg_graph_generate_chunglu",
     "mg_graph_from_mtx_ex", "mg_csr_from_mtx", "mg_csr_info", "mg_csr_arrays", "mg_csr_free",
-    "mg_result_level_map",
+    "mg_result_level_map", "mg_result_level_csr",
 ]
 TUNE_OFF, TUNE_CACHED, TUNE_ON = 0, 1, 2
 LOAD_CACHE_READ, LOAD_CACHE_WRITE = 1, 2
@@ -166,6 +166,7 @@ def lib():
     L.mg_result_level_sizes.argtypes = [vp, vp, i32, ct.POINTER(i32)]
     L.mg_result_trace.argtypes = [vp, vp, i32, ct.POINTER(i32)]
     L.mg_result_level_map.argtypes = [vp, i32, vp, u32, ct.POINTER(u32)]
+    L.mg_result_level_csr.argtypes = [vp, i32, ct.POINTER(u32), ct.POINTER(u64), vp, vp, vp]
     L.mg_result_destroy.argtypes = [vp]
     L.mg_batch_draw_sbm_params.argtypes = [u32, u32, u32, u32, u32, dbl, dbl, dbl, dbl, u64, vp]
     L.mg_batch_generate_sbm.argtypes = [vp, u32, vp, pp]
@@ -638,9 +639,11 @@ class Graph:
         return cd[:n], Graph(self.ctx, h)
 
     def louvain(self, version: int = 2, threshold: float = 1e-6, max_phases: int = 1000,
-                precision: str = "fp64", verbose: bool = False, keep_levels: bool = False) -> dict:
-        """mg_louvain_run; with keep_levels the result also holds "level_maps",
-        the dendrogram (one community map per level, mg_result_level_map)."""
+                precision: str = "fp64", verbose: bool = False, keep_levels: int = 0) -> dict:
+        """mg_louvain_run; with keep_levels >= 1 the result also holds
+        "level_maps", the dendrogram (one community map per level,
+        mg_result_level_map); with keep_levels = 2 also "level_csr", the
+        (offsets, cols, weights) of the graph every level worked on."""
         opts = _RunOpts(version, threshold, max_phases, _PREC[precision], int(verbose), int(keep_levels))
         r = ct.c_void_p()
         self.ctx.check(lib().mg_louvain_run(self.h, ct.byref(opts), ct.byref(r)), "mg_louvain_run")
@@ -671,6 +674,18 @@ class Graph:
                     lib().mg_result_level_map(r, lvl, _p(m), size.value, ct.byref(size))
                     maps.append(m[: size.value])
                 out["level_maps"] = maps
+            if keep_levels >= 2:
+                graphs = []
+                for lvl in range(s.levels):
+                    ln, lm = ct.c_uint32(), ct.c_uint64()
+                    if lib().mg_result_level_csr(r, lvl, ct.byref(ln), ct.byref(lm), None, None, None) != MG_OK:
+                        break
+                    off = np.zeros(ln.value + 1, np.uint64)
+                    cols = np.zeros(max(lm.value, 1), np.uint32)
+                    w = np.zeros(max(lm.value, 1), np.float64)
+                    lib().mg_result_level_csr(r, lvl, ct.byref(ln), ct.byref(lm), _p(off), _p(cols), _p(w))
+                    graphs.append((off, cols[: lm.value], w[: lm.value]))
+                out["level_csr"] = graphs
             return out
         finally:
             lib().mg_result_destroy(r)

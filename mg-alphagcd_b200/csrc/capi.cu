@@ -535,6 +535,20 @@ mg_status mg_result_level_map(const mg_result *r, int level, uint32_t *out, uint
     return MG_OK;
 }
 
+mg_status mg_result_level_csr(const mg_result *r, int level, uint32_t *n, uint64_t *nnz, uint64_t *offsets,
+                              uint32_t *cols, double *weights) {
+    if (!r || level < 0 || level >= (int)r->level_csr.size()) return MG_ERR_INVALID;
+    const mg_result::LevelCsr &L = r->level_csr[(size_t)level];
+    const uint32_t nn = (uint32_t)(L.off.size() - 1);
+    if (n) *n = nn;
+    if (nnz) *nnz = L.col.size();
+    if (offsets)
+        for (size_t i = 0; i < L.off.size(); i++) offsets[i] = L.off[i];
+    if (cols && !L.col.empty()) memcpy(cols, L.col.data(), sizeof(uint32_t) * L.col.size());
+    if (weights && !L.w.empty()) memcpy(weights, L.w.data(), sizeof(double) * L.w.size());
+    return MG_OK;
+}
+
 mg_status mg_result_trace(const mg_result *r, double *rows4, int max_rows, int *count) {
     if (!r) return MG_ERR_INVALID;
     int c = (int)(r->trace.size() / 4);

@@ -54,6 +54,13 @@ struct mg_result {
     std::vector<uint32_t> level_sizes;
     std::vector<double> trace;  // rows of 4
     std::vector<std::vector<uint32_t>> level_maps;  // dendrogram (keep_levels)
+    // the graph every level worked on (keep_levels >= 2): offsets, columns,
+    // weights as double
+    struct LevelCsr {
+        std::vector<uint32_t> off, col;
+        std::vector<double> w;
+    };
+    std::vector<LevelCsr> level_csr;
 };
 
 namespace mg {

@@ -60,6 +60,25 @@ void print_phase_header(int phase) {
 
 }  // namespace
 
+// Host copy of the graph a level works on (opt-in: keep_levels >= 2).
+void keep_level_csr(const GraphView &cur, mg_result &res, cudaStream_t s) {
+    res.level_csr.emplace_back();
+    mg_result::LevelCsr &L = res.level_csr.back();
+    L.off.resize((size_t)cur.n + 1);
+    L.col.resize(cur.nnz);
+    L.w.assign(cur.nnz, 1.0);
+    MG_CUDA(cudaMemcpyAsync(L.off.data(), cur.off, sizeof(uint32_t) * ((size_t)cur.n + 1), cudaMemcpyDeviceToHost, s));
+    if (cur.nnz) MG_CUDA(cudaMemcpyAsync(L.col.data(), cur.col, sizeof(uint32_t) * cur.nnz, cudaMemcpyDeviceToHost, s));
+    if (cur.nnz && cur.wk == WK_F64) {
+        MG_CUDA(cudaMemcpyAsync(L.w.data(), cur.w, sizeof(double) * cur.nnz, cudaMemcpyDeviceToHost, s));
+    } else if (cur.nnz && cur.wk == WK_F32) {
+        std::vector<float> w32(cur.nnz);
+        MG_CUDA(cudaMemcpyAsync(w32.data(), cur.w, sizeof(float) * cur.nnz, cudaMemcpyDeviceToHost, s));
+        MG_CUDA(cudaStreamSynchronize(s));
+        for (uint64_t e = 0; e < cur.nnz; e++) L.w[e] = w32[e];
+    }
+}
+
 void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result &res) {
     ctx_prepare(ctx);
     cudaStream_t s = ctx->stream;
@@ -105,6 +124,7 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
         const uint32_t n = cur.n;
         res.level_sizes.push_back(n);
         S.levels++;
+        if (o.keep_levels >= 2) keep_level_csr(cur, res, s);
         if (verbose) print_phase_header(phase);
         double phase_lm = 0;
         Timer tp(ctx->ev[0], ctx->ev[1], s);

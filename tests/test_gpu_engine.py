@@ -325,3 +325,23 @@ def test_dendrogram_levels_compose_to_assignment(O, ctx):
         assert (comp == a["assignment"]).all()
         assert (a["assignment"] == O.louvain(g)["assignment"]).all()
         assert "level_maps" not in dg.louvain()
+
+
+def test_level_graphs_equal_oracle_coarsening(O, ctx):
+    """keep_levels = 2: the graph of every level; level 0 is the input, level
+    l + 1 is the oracle's coarsening of level l by level l's map (bit-exact)."""
+    g = O.gen_rmat(14, seed=2)
+    dg = _up(ctx, g)
+    a = dg.louvain(keep_levels=2)
+    graphs, maps = a["level_csr"], a["level_maps"]
+    assert len(graphs) == len(maps) == a["levels"]
+    off, cols, w = graphs[0]
+    assert (off == g.offsets).all() and (cols == g.cols).all() and (w == 1).all()
+    cur = g
+    for lvl in range(len(graphs) - 1):
+        _, h, _ = O.coarsen(cur, maps[lvl])
+        off, cols, w = graphs[lvl + 1]
+        assert len(off) - 1 == a["level_sizes"][lvl + 1]
+        assert (off == h.offsets).all() and (cols == h.cols).all() and (w == h.weights).all(), lvl
+        cur = h
+    assert "level_csr" not in dg.louvain(keep_levels=1)
