@@ -38,7 +38,10 @@ latency percentiles measure service, not backlog.
 
 --impl reference times the reference's Louvain logic on the host cores (the
 CPU oracle port under OpenMP, all host threads): each step is one phase-0
-sweep (local move + sigma update + modularity) over the same graph.
+sweep (local move + sigma update + modularity) over the same graph, and one
+full run to convergence beside the steps gives its time to solution and Q.
+The engine arm runs the same full oracle run on the graph it timed
+("cpu_baseline.full_run") and reports |Q - Q_oracle|.
 Multi-GPU runs are independent replicas (a single graph does not shard).
 """
 from __future__ import annotations
@@ -70,6 +73,8 @@ def parse():
     ap.add_argument("--scale", type=int, default=RMAT["scale"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-full-run", dest="full_run", action="store_false",
+                    help="skip the oracle's full run to convergence (Q_oracle, time to solution)")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-graphs", type=int, default=4096)
     ap.add_argument("--batch-steps", type=int, default=2)
@@ -217,11 +222,22 @@ def cpu_baseline_sample(csr, threads):
     return edges / t, t
 
 
-def rmat_config(scale, n, nnz, parallelism):
-    """The workload description both arms report."""
+def rmat_config(scale, n, nnz):
+    """The workload description both arms report (identical dicts)."""
     return {"workload": f"rmat{scale}_ef16_louvain_full", "vertices": n, "directed_entries": nnz,
             "abcd": [RMAT["a"], RMAT["b"], RMAT["c"], 0.05], "seed": RMAT["seed"],
-            "l2": "inputs larger than L2 (2.1 GB of column ids)", "parallelism": parallelism}
+            "l2": "inputs larger than L2 (2.1 GB of column ids)"}
+
+
+def oracle_full_run(O, csr):
+    """The oracle's Louvain to convergence (version 2, threshold 1e-6) on the
+    host cores: time to solution, Q, levels and iterations."""
+    t0 = time.perf_counter()
+    r = O.louvain(csr)
+    t = time.perf_counter() - t0
+    return {"seconds": t, "modularity": r["modularity"], "levels": [int(x) for x in r["level_sizes"]],
+            "iterations": int(r["iterations"]), "communities": int(r["communities"]),
+            "threads": O.get_threads()}
 
 
 def run_reference(args, world, rank, local, pg):
@@ -243,15 +259,22 @@ def run_reference(args, world, rank, local, pg):
     v = tot_e / tot_t
     sample = (f"one phase-0 sweep (local move + sigma update + modularity) per step over the full "
               f"R-MAT-{args.scale} graph ({g.nnz} directed entries), version 2")
+    full = oracle_full_run(O, g) if args.full_run else None
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded R-MAT generator)",
-        "config": rmat_config(args.scale, g.n, g.nnz, f"host threads ({threads})"),
+        "config": rmat_config(args.scale, g.n, g.nnz),
+        "parallelism": f"host threads ({threads})",
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        # time to solution beside the sweep samples: one run to convergence
+        "full_run": full,
     }
+    if full is not None:
+        line["convergence_s"] = full["seconds"]
+        line["modularity"] = full["modularity"]
     return line
 
 
@@ -261,41 +284,88 @@ def _timed_runs(g, k, **kw):
     return runs, statistics.median(r["seconds_total"] for r in runs)
 
 
-def run_sbm64k(ctx):
+def run_sbm64k(ctx, with_oracle=True):
     g = ctx.generate_sbm(65536, 64, 16.0, 0.8, 1)
     info = g.info()
     runs, t = _timed_runs(g, 3)
     r = runs[-1]
+    ref = None
+    if with_oracle:
+        O = _oracle()
+        off, cols, _ = g.csr()
+        ref = oracle_full_run(O, O.CSR(len(off) - 1, off, cols, None))
     g.close()
-    return {"workload": "SBM 65,536 vertices, 64 blocks, mean degree 16, 80% intra, seed 1, unit weights",
-            "directed_entries": info["nnz"], "modularity": r["modularity"], "communities": r["communities"],
-            "vertices_per_level": [int(x) for x in r["level_sizes"]], "phases": r["phases"],
-            "iterations": r["iterations"], "run_s": t, "edges_per_s": r["edges_swept"] / r["seconds_total"]}
+    out = {"workload": "SBM 65,536 vertices, 64 blocks, mean degree 16, 80% intra, seed 1, unit weights",
+           "directed_entries": info["nnz"], "modularity": r["modularity"], "communities": r["communities"],
+           "vertices_per_level": [int(x) for x in r["level_sizes"]], "phases": r["phases"],
+           "iterations": r["iterations"], "run_s": t, "edges_per_s": r["edges_swept"] / r["seconds_total"]}
+    if ref is not None:
+        out["oracle"] = ref
+        out["abs_error_vs_oracle"] = abs(r["modularity"] - ref["modularity"])
+        out["levels_equal_oracle"] = out["vertices_per_level"] == ref["levels"]
+    return out
 
 
-def run_precision(ctx):
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as O
+
+    O.set_threads(os.cpu_count() or 1)
+    return O
+
+
+def run_precision(ctx, with_oracle=True):
+    """Chung-Lu 4M: FP32 gains (FP64 sigma and Q) and FP64 gains on the
+    lognormal weights, FP64 and exact int64 gains on the unit-weight copy.
+    Each result's error is stated against the FP64 oracle twice: Q
+    recomputed by the oracle from the returned assignment (the reported
+    number's own error) and the oracle's own FP64 run to convergence on the
+    same graph (the algorithm's error)."""
+    import numpy as np
+
     n = 4_194_304
+    O = _oracle() if with_oracle else None
+
+    def one(g, runs, t, prec, csr, ref):
+        r = runs[-1]
+        out = {"precision": prec, "modularity": r["modularity"], "run_s": t, "levels": len(r["level_sizes"])}
+        if O is not None:
+            qo = O.modularity(csr, r["assignment"])
+            out["modularity_oracle_fp64_from_assignment"] = qo
+            out["abs_error_vs_oracle_recomputed"] = abs(r["modularity"] - qo)
+            out["abs_error_vs_oracle_run"] = abs(r["modularity"] - ref["modularity"])
+        return out
+
+    def oracle_run(g):
+        if O is None:
+            return None, None
+        off, cols, w = g.csr()
+        csr = O.CSR(len(off) - 1, off, cols, None if bool(np.all(w == 1.0)) else w)
+        return csr, oracle_full_run(O, csr)
+
     gw = ctx.generate_chunglu(n, 2.1, 20.0, 200000.0, lognormal=True, seed=3)
     info = gw.info()
+    csr_w, ref_w = oracle_run(gw)
     r64, t64 = _timed_runs(gw, 2, precision="fp64")
     r32, t32 = _timed_runs(gw, 2, precision="fp32")
-    q64, q32 = r64[-1]["modularity"], r32[-1]["modularity"]
-    q32_fp64 = gw.modularity(r32[-1]["assignment"])
+    w64 = one(gw, r64, t64, "fp64", csr_w, ref_w)
+    w32 = one(gw, r32, t32, "fp32", csr_w, ref_w)
     gw.close()
+    del csr_w
     gu = ctx.generate_chunglu(n, 2.1, 20.0, 200000.0, lognormal=False, seed=3)
+    csr_u, ref_u = oracle_run(gu)
     u64, tu64 = _timed_runs(gu, 2, precision="fp64")
     ui, tui = _timed_runs(gu, 2, precision="int64")
+    x64 = one(gu, u64, tu64, "fp64", csr_u, ref_u)
+    xi = one(gu, ui, tui, "int64", csr_u, ref_u)
     gu.close()
+    del csr_u
     return {"workload": "Chung-Lu 4,194,304 vertices, exponent 2.1, mean degree 20, max degree 200,000, seed 3",
             "directed_entries": info["nnz"],
-            "lognormal_f32_weights": {"fp64": {"modularity": q64, "run_s": t64},
-                                      "fp32": {"modularity": q32, "run_s": t32,
-                                               "modularity_recomputed_fp64": q32_fp64},
-                                      "fp32_vs_fp64_abs_error": abs(q32 - q64),
-                                      "fp32_reported_vs_recomputed_abs_error": abs(q32 - q32_fp64)},
-            "unit_weights": {"fp64": {"modularity": u64[-1]["modularity"], "run_s": tu64},
-                             "int64": {"modularity": ui[-1]["modularity"], "run_s": tui},
-                             "int64_vs_fp64_abs_error": abs(ui[-1]["modularity"] - u64[-1]["modularity"]),
+            "lognormal_f32_weights": {"fp64": w64, "fp32": w32, "oracle_fp64_run": ref_w,
+                                      "fp32_vs_fp64_abs_error": abs(w32["modularity"] - w64["modularity"])},
+            "unit_weights": {"fp64": x64, "int64": xi, "oracle_fp64_run": ref_u,
+                             "int64_vs_fp64_abs_error": abs(xi["modularity"] - x64["modularity"]),
                              "same_assignment": bool((ui[-1]["assignment"] == u64[-1]["assignment"]).all())}}
 
 
@@ -520,24 +590,23 @@ def run_engine(args, world, rank, local, pg):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        import types
-
-        csr = types.SimpleNamespace(n=info["n"], offsets=off, cols=cols, weights=None)
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle_py as O
-
+        O = _oracle()
         threads = os.cpu_count() or 1
         cg = O.CSR(info["n"], off, cols, None)
         cv, ct_ = cpu_baseline_sample(cg, threads)
         cpu = {"value": cv, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"one phase-0 sweep (local move + sigma update + modularity) over the same graph, "
                          f"{ct_:.1f} s on {threads} threads"}
-        del csr
+        if args.full_run:
+            # the oracle to convergence on the graph the engine ran: Q_oracle
+            # and its time to solution
+            cpu["full_run"] = oracle_full_run(O, cg)
+        del cg
     batched = serving = sbm64k = precision = loader = None
     if world == 1 and not args.no_extra:
         g.close()
-        sbm64k = run_sbm64k(ctx)
-        precision = run_precision(ctx)
+        sbm64k = run_sbm64k(ctx, with_oracle=not args.no_cpu_baseline)
+        precision = run_precision(ctx, with_oracle=not args.no_cpu_baseline)
         loader = run_loader(mg, ctx)
     if world == 1 and not args.no_batched:
         g.close()
@@ -558,7 +627,8 @@ def run_engine(args, world, rank, local, pg):
         "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded R-MAT generator, graph built on the device)",
-        "config": rmat_config(args.scale, info["n"], info["nnz"], "replicas" if world > 1 else "single GPU"),
+        "config": rmat_config(args.scale, info["n"], info["nnz"]),
+        "parallelism": f"replicas ({world} GPUs)" if world > 1 else "single GPU",
         "modularity": last["modularity"], "communities": last["communities"],
         "levels": [int(x) for x in last["level_sizes"]], "iterations": last["iterations"],
         "first_pass_edges_per_s": last["phase0_edges_swept"] / last["phase0_seconds"],
@@ -571,6 +641,13 @@ def run_engine(args, world, rank, local, pg):
                      "kernel": "local-move sweep (all bins)", "peak_kind": peak_kind,
                      "sweeps": sweeps, "algorithmic_bytes_per_sweep": sweep_b / max(sweeps, 1)},
         "cpu_baseline": cpu,
+        "modularity_vs_oracle": None if not (cpu and cpu.get("full_run")) else {
+            "q_oracle": cpu["full_run"]["modularity"],
+            "abs_error": abs(last["modularity"] - cpu["full_run"]["modularity"]),
+            "levels_equal": [int(x) for x in last["level_sizes"]] == cpu["full_run"]["levels"],
+            "iterations_equal": last["iterations"] == cpu["full_run"]["iterations"],
+            "oracle_convergence_s": cpu["full_run"]["seconds"],
+            "engine_convergence_s": last["seconds_total"]},
         "e2e": None if args.e2e_steps <= 0 else {"value": e2e_esum / e2e_tmax, "unit": UNIT,
                 "h2d_bytes_per_step": 8 * (info["n"] + 1) + 4 * info["nnz"],
                 "d2h_bytes_per_step": 4 * info["n"]},

@@ -167,13 +167,14 @@ mg_status mg_local_move(mg_graph *g, int version, int up, int precision, const u
  * weights d_k (n each) and the output d_C_new (n).  mass = sum of all
  * weights.  Results equal mg_local_move (FP64 gains) for integral weights.
  * Work is queued on `stream` (a cudaStream_t, NULL = default stream); the call
- * waits for the stream once, to read the graph's maximum degree.
+ * waits for the stream once, to read the graph's maximum degree, so it must
+ * not be called while that stream is being captured into a CUDA graph.
  * Scratch: the per-block hash tables live in one static 16 MiB device array
- * that every GPU loading the library holds until exit.  A graph whose
- * maximum degree needs a table beyond it (a degree above 524,287) is rejected
- * with MG_ERR_UNSUPPORTED.  The first call on a device looks up
- * that array's device address (a one-time set-up per device); make that first
- * call before any stream capture.  All calls share the array and clear it on
+ * that every GPU loading the library holds until exit; each vertex uses a
+ * table sized by its own degree.  A graph whose maximum degree needs a table
+ * beyond it (a degree above 524,287) is rejected with MG_ERR_UNSUPPORTED.
+ * The first call on a device looks up that array's device address (a
+ * one-time set-up per device).  All calls share the array and clear it on
  * entry, so calls that overlap on the GPU race with each other.  Errors are
  * reported by mg_last_error(NULL). */
 mg_status mg_local_move_noalloc(uint32_t n, const uint32_t *d_offsets, const uint32_t *d_cols,
@@ -272,6 +273,26 @@ mg_status mg_tune_table(mg_ctx *ctx, char *buf, size_t cap, size_t *len);
 /* Save / load the table (same text). Loading merges into the context's table. */
 mg_status mg_tune_save(mg_ctx *ctx, const char *path);
 mg_status mg_tune_load(mg_ctx *ctx, const char *path);
+
+/* ---- heavy-vertex policy ----------------------------------------------------------
+ * Where the reference sends every vertex above degree 4094 to one global-table
+ * kernel (calculate_eicj_and_move_vertex_gl_bk, src/louvain/louvain.cu:810-1030,
+ * dispatched at :1257-1285), the engine splits them by degree class: classes
+ * 13..17 (degree 4,097..131,072) go to thread-block-cluster tables of 1..16 CTAs,
+ * class 18 (above 131,072) to global-memory tables.  Every choice below gives
+ * the same result (bit for bit on integral weights); they exist for tuning and
+ * so that tests can force each path. */
+enum {
+    MG_FILL_AUTO = 0,  /* own fill on a phase's first sweep, split fill once communities repeat */
+    MG_FILL_OWN = 1,   /* every CTA of a cluster reads the whole row and inserts the communities it owns */
+    MG_FILL_SPLIT = 2  /* the CTAs split the row; equal communities combined in the warp; inserts via DSMEM */
+};
+typedef struct {
+    int cluster_fill; /* MG_FILL_* */
+    int giant_class;  /* degree classes >= this (13..18) take the global-table path; 0 = default (18) */
+} mg_sweep_opts;
+/* Set the context's policy (opts NULL = defaults); applies to later sweeps and runs. */
+mg_status mg_sweep_options(mg_ctx *ctx, const mg_sweep_opts *opts);
 
 /* ---- batched form --------------------------------------------------------------
  * No reference counterpart: the reference runs one graph per process.  A batch

@@ -48,6 +48,10 @@ class _Opts(ct.Structure):
     _fields_ = [("device", ct.c_int), ("verbose", ct.c_int), ("hbm_budget_bytes", ct.c_size_t)]
 
 
+class _SweepOpts(ct.Structure):
+    _fields_ = [("cluster_fill", ct.c_int), ("giant_class", ct.c_int)]
+
+
 class _RunOpts(ct.Structure):
     _fields_ = [("version", ct.c_int), ("threshold", ct.c_double), ("max_phases", ct.c_int),
                 ("precision", ct.c_int), ("verbose", ct.c_int), ("keep_levels", ct.c_int)]
@@ -116,9 +120,10 @@ EXPORTED = [
     "mg_serve_cancel", "mg_serve_release", "mg_serve_stats", "mg_serve_last_error", "mg_serve_stop",
     "mg_tune_mode", "mg_tune_table", "mg_tune_save", "mg_tune_load", "mg_graph_generate_chunglu",
     "mg_graph_from_mtx_ex", "mg_csr_from_mtx", "mg_csr_info", "mg_csr_arrays", "mg_csr_free",
-    "mg_result_level_map", "mg_result_level_csr",
+    "mg_result_level_map", "mg_result_level_csr", "mg_sweep_options",
 ]
 TUNE_OFF, TUNE_CACHED, TUNE_ON = 0, 1, 2
+FILL_AUTO, FILL_OWN, FILL_SPLIT = 0, 1, 2
 LOAD_CACHE_READ, LOAD_CACHE_WRITE = 1, 2
 
 
@@ -181,6 +186,7 @@ def lib():
     L.mg_batch_result_destroy.argtypes = [vp]
     L.mg_batch_generate.argtypes = [vp, u32, vp, pp]
     L.mg_tune_mode.argtypes = [vp, i32]
+    L.mg_sweep_options.argtypes = [vp, ct.POINTER(_SweepOpts)]
     L.mg_tune_table.argtypes = [vp, ct.c_char_p, ct.c_size_t, ct.POINTER(ct.c_size_t)]
     L.mg_tune_save.argtypes = [vp, ct.c_char_p]
     L.mg_tune_load.argtypes = [vp, ct.c_char_p]
@@ -298,6 +304,13 @@ class Context:
     def tune_mode(self, mode: int):
         """TUNE_OFF: built-in shapes; TUNE_CACHED: table only; TUNE_ON: also time new classes."""
         self.check(lib().mg_tune_mode(self.h, mode), "mg_tune_mode")
+
+    def sweep_options(self, cluster_fill: int = FILL_AUTO, giant_class: int = 0):
+        """Heavy-vertex policy (mg_sweep_options): the cluster-table fill
+        (FILL_*) and the first degree class (13..18, 0 = default) sent to the
+        global-table path.  Results do not depend on it."""
+        o = _SweepOpts(cluster_fill, giant_class)
+        self.check(lib().mg_sweep_options(self.h, ct.byref(o)), "mg_sweep_options")
 
     def tune_table(self) -> list:
         """Entries: (weight kind, precision, version, batched, class, size bucket, shape, microseconds)."""

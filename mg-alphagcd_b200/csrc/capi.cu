@@ -395,6 +395,7 @@ mg_status mg_local_move(mg_graph *g, int version, int up, int precision, const u
         sp.precision = precision;
         sp.mass = g->mass;
         sp.integral = g->integral;
+        sp.agg = sweep_agg(ctx->mws, 0);
         sweep_reset_acc(ctx->mws, s);
         move_sweep(g->view(), lvl, ctx->mws, sp, dC, dN, dk, ds, s);
         MG_CUDA(cudaMemcpyAsync(C_new, dN, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
@@ -465,8 +466,13 @@ mg_status mg_coarsen(mg_graph *g, const uint32_t *C, uint32_t *C_dense, mg_graph
         std::swap(ng->off.cap, lv.off.cap);
         std::swap(ng->col.p, lv.col.p);
         std::swap(ng->col.cap, lv.col.cap);
-        std::swap(ng->w64.p, lv.w.p);
-        std::swap(ng->w64.cap, lv.w.cap);
+        if (lv.wk == WK_U32) {
+            level_weights_f64(lv.view(), ng->w64.ensure(lv.nnz + 1), s);
+            MG_CUDA(cudaStreamSynchronize(s));
+        } else {
+            std::swap(ng->w64.p, lv.w.p);
+            std::swap(ng->w64.cap, lv.w.cap);
+        }
         ng->wk = WK_F64;
         ng->mass = g->mass;
         ng->integral = g->integral;
@@ -584,6 +590,18 @@ mg_status mg_tune_mode(mg_ctx *ctx, int mode) {
     if (!ctx) return MG_ERR_INVALID;
     if (mode < MG_TUNE_OFF || mode > MG_TUNE_ON) return fail(ctx, MG_ERR_INVALID, "mg_tune_mode: unknown mode");
     ctx->mws.tune.mode = mode;
+    return MG_OK;
+}
+
+mg_status mg_sweep_options(mg_ctx *ctx, const mg_sweep_opts *opts) {
+    if (!ctx) return MG_ERR_INVALID;
+    const int fill = opts ? opts->cluster_fill : MG_FILL_AUTO;
+    const int gc = opts && opts->giant_class ? opts->giant_class : kFirstHeavyClass + kTiers - 1;
+    if (fill < MG_FILL_AUTO || fill > MG_FILL_SPLIT) return fail(ctx, MG_ERR_INVALID, "mg_sweep_options: unknown fill");
+    if (gc < kFirstHeavyClass || gc > kFirstHeavyClass + kTiers - 1)
+        return fail(ctx, MG_ERR_INVALID, "mg_sweep_options: giant_class must be 0 or 13..18");
+    ctx->mws.cluster_fill = fill;
+    ctx->mws.giant_class = gc;
     return MG_OK;
 }
 

@@ -132,6 +132,7 @@ __global__ void __launch_bounds__(kExpandThreads) expand_keys_kernel(const uint3
                 keys[e] = ((uint64_t)Cd[rowat[q + (q >> 5)]] << bc) | Cd[__ldcs(col + e)];
                 if constexpr (WK == WK_F32) vals[e] = (PV)__ldcs((const float *)w + e);
                 else if constexpr (WK == WK_F64) vals[e] = (PV)__ldcs((const double *)w + e);
+                else if constexpr (WK == WK_U32) vals[e] = (PV)__ldcs((const uint32_t *)w + e);
             }
         }
         __syncthreads();  // rowat is reused by the next tile
@@ -179,10 +180,11 @@ void emit_rows(const uint64_t *ukey, uint32_t u, int bc, uint32_t n_rows, uint32
                cudaStream_t s);
 
 // run weights as run lengths (unit weights)
-__global__ void run_lengths_kernel(const uint32_t *ustart, uint32_t u, uint32_t m, double *w) {
+template <class W>
+__global__ void run_lengths_kernel(const uint32_t *ustart, uint32_t u, uint32_t m, W *w) {
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < u; s += gridDim.x * blockDim.x) {
         uint32_t end = s + 1 < u ? ustart[s + 1] : m;
-        w[s] = (double)(end - ustart[s]);
+        w[s] = (W)(end - ustart[s]);
     }
 }
 
@@ -192,11 +194,17 @@ __global__ void to_u64_kernel(const T *v, size_t m, uint64_t *o) {
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x)
         o[i] = (uint64_t)v[i];
 }
-__global__ void run_diff_kernel(const uint32_t *ustart, uint32_t u, uint32_t m, const uint64_t *pre, double *w) {
+// (the sums of an integral graph are below its mass < 2^32: exact as uint32)
+__global__ void run_diff_kernel(const uint32_t *ustart, uint32_t u, uint32_t m, const uint64_t *pre, uint32_t *w) {
     for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < u; s += gridDim.x * blockDim.x) {
         uint32_t end = s + 1 < u ? ustart[s + 1] : m;
-        w[s] = (double)(pre[end] - pre[ustart[s]]);
+        w[s] = (uint32_t)(pre[end] - pre[ustart[s]]);
     }
+}
+
+__global__ void u32_to_f64_kernel(const uint32_t *a, uint64_t m, double *o) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x)
+        o[i] = (double)a[i];
 }
 
 // real weights: each thread sums 8 consecutive sorted entries run by run and
@@ -307,6 +315,17 @@ uint32_t unique_runs(const uint64_t *keys, size_t m, int bc, uint32_t n_rows, Le
 
 }  // namespace
 
+void level_weights_f64(const GraphView &g, double *out, cudaStream_t s) {
+    if (g.nnz == 0) return;
+    if (g.wk == WK_F64) {
+        MG_CUDA(cudaMemcpyAsync(out, g.w, sizeof(double) * g.nnz, cudaMemcpyDeviceToDevice, s));
+        return;
+    }
+    MG_CHECK(g.wk == WK_U32, MG_ERR_INVALID, "level_weights_f64: unexpected weight kind");
+    u32_to_f64_kernel<<<grid_for(g.nnz), 256, 0, s>>>((const uint32_t *)g.w, g.nnz, out);
+    MG_LAUNCH_CHECK();
+}
+
 uint32_t relabel_dense(const uint32_t *C, uint32_t n, uint32_t *C_dense, CoarsenWorkspace &ws, cudaStream_t s) {
     if (n == 0) return 0;
     uint32_t *flags = ws.flags.ensure((size_t)n + 1);
@@ -333,12 +352,15 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
         MG_LAUNCH_CHECK();
         exclusive_scan<uint64_t>(upper_degree_off, upper_degree_off, n_new, upper_degree_off + n_new, s, ws.prim);
     }
+    // integral graphs: the next level's weights as exact 32-bit integers
+    out.wk = integral ? WK_U32 : WK_F64;
     if (m == 0) {
         out.n = n_new;
         out.nnz = 0;
         MG_CUDA(cudaMemsetAsync(out.off.ensure((size_t)n_new + 1), 0, sizeof(uint32_t) * ((size_t)n_new + 1), s));
         out.col.ensure(1);
         out.w.ensure(1);
+        out.wi.ensure(1);
         return;
     }
     uint64_t *keys = ws.keys.ensure(m);
@@ -358,6 +380,8 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
             expand_keys_kernel<WK_UNIT, PV><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
         else if (g.wk == WK_F32)
             expand_keys_kernel<WK_F32, PV><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
+        else if (g.wk == WK_U32)
+            expand_keys_kernel<WK_U32, PV><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
         else expand_keys_kernel<WK_F64, PV><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
         MG_LAUNCH_CHECK();
     };
@@ -371,9 +395,11 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
     const double *sv = flipped ? vals2 : vals;
     uint32_t *ustart, *seg, *head;
     uint32_t u = unique_runs(sk, m, bc, n_new, out, ws, s, &ustart, &seg, &head);
-    double *w = out.w.ensure(u + 1);
-    if (!weighted) {
-        run_lengths_kernel<<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)m, w);
+    if (integral && !weighted) {
+        run_lengths_kernel<uint32_t><<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)m, out.wi.ensure(u + 1));
+        MG_LAUNCH_CHECK();
+    } else if (!weighted) {
+        run_lengths_kernel<double><<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)m, out.w.ensure(u + 1));
         MG_LAUNCH_CHECK();
     } else if (integral) {
         // exact: 64-bit prefix sums over the sorted weights, run sum = difference
@@ -381,9 +407,10 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
         to_u64_kernel<uint32_t><<<grid_for(m), 256, 0, s>>>(flipped ? ivals2 : ivals, m, pre);
         MG_LAUNCH_CHECK();
         exclusive_scan<uint64_t>(pre, pre, m, pre + m, s, ws.prim);
-        run_diff_kernel<<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)m, pre, w);
+        run_diff_kernel<<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)m, pre, out.wi.ensure(u + 1));
         MG_LAUNCH_CHECK();
     } else {
+        double *w = out.w.ensure(u + 1);
         MG_CUDA(cudaMemsetAsync(w, 0, sizeof(double) * u, s));
         run_sums_kernel<<<(unsigned)ceil_div(ceil_div(m, kSegItems), 256), 256, 0, s>>>(sv, m, seg, head, w);
         MG_LAUNCH_CHECK();
@@ -394,6 +421,7 @@ void csr_from_device_pairs(uint32_t n, uint64_t m, const uint32_t *u, const uint
                            CoarsenWorkspace &ws, cudaStream_t s, const double *w) {
     const size_t mm = 2 * m;
     MG_CHECK(mm < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "graph has more than 2^32-1 directed entries");
+    out.wk = WK_F64;
     if (m == 0) {
         out.n = n;
         out.nnz = 0;

@@ -44,13 +44,16 @@ extern thread_local unsigned long long g_kernel_launches;
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
 constexpr int kNumSMs = 148;
 
-enum WeightKind { WK_UNIT = 0, WK_F32 = 1, WK_F64 = 2 };
+// WK_U32: exact 32-bit integer weights, the storage of every coarsened level
+// of an integral graph (each coarsened weight is at most the graph's mass,
+// which is below 2^32 for integral graphs): 4 bytes per entry instead of 8.
+enum WeightKind { WK_UNIT = 0, WK_F32 = 1, WK_F64 = 2, WK_U32 = 5 };
 // Kernel variants: weights stored as f32 / f64 whose values are integral
-// (every coarsened level of an integral graph) accumulate in 32-bit integer
-// table slots, which shared and distributed shared memory add natively.
+// accumulate in 32-bit integer table slots, which shared and distributed
+// shared memory add natively.
 enum { WK_F32I = 3, WK_F64I = 4 };
 template <int WK>
-constexpr bool kIntg = WK == WK_UNIT || WK == WK_F32I || WK == WK_F64I;
+constexpr bool kIntg = WK == WK_UNIT || WK == WK_F32I || WK == WK_F64I || WK == WK_U32;
 
 inline uint64_t ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
 inline uint32_t pow2_at_least(uint64_t x, uint32_t lo = 16) {

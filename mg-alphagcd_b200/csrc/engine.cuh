@@ -122,6 +122,10 @@ struct MoveWorkspace {
     DBuf<uint32_t> perm;
     DBuf<uint2> rows;              // {off[perm[q]], off[perm[q] + 1]} per class-list entry q
     int max_cluster = 0;           // largest cluster size the device runs (8 or 16)
+    // heavy-vertex policy (mg_sweep_options): first degree class worked by the
+    // global-table path (13..18), and the cluster-table fill (MG_FILL_*)
+    int giant_class = kFirstHeavyClass + kTiers - 1;
+    int cluster_fill = MG_FILL_AUTO;
     // heavy-vertex global tables
     DBuf<uint64_t> h_toff;         // table offset per heavy vertex (H+1)
     DBuf<uint32_t> h_tsize;        // table size per heavy vertex
@@ -157,6 +161,10 @@ struct SweepParams {
     // first sweep of a phase, where every community is one vertex).
     int agg = 0;
 };
+// the agg flag of a sweep: the automatic choice unless the workspace forces a fill
+inline int sweep_agg(const MoveWorkspace &ws, int automatic) {
+    return ws.cluster_fill == MG_FILL_OWN ? 0 : ws.cluster_fill == MG_FILL_SPLIT ? 1 : automatic;
+}
 
 // Constants of the gain of one graph, from its mass (sum of all directed
 // weights): m = mass/2 and the correctly rounded reciprocals the exact
@@ -238,22 +246,28 @@ struct CoarsenWorkspace {
     DBuf<uint32_t> u32tmp;
     PrimWorkspace prim;
 };
+// A device CSR level: f64 weights (w, wk = WK_F64), or exact 32-bit integer
+// weights (wi, wk = WK_U32) for the coarsened levels of integral graphs.
 struct LevelGraph {
     uint32_t n = 0;
     uint64_t nnz = 0;
     DBuf<uint32_t> off, col;
     DBuf<double> w;
+    DBuf<uint32_t> wi;
+    int wk = WK_F64;
     GraphView view() const {
         GraphView v;
         v.n = n;
         v.nnz = nnz;
         v.off = off.get();
         v.col = col.get();
-        v.w = w.get();
-        v.wk = WK_F64;
+        v.w = wk == WK_U32 ? (const void *)wi.get() : (const void *)w.get();
+        v.wk = wk;
         return v;
     }
 };
+// The weights of a level as doubles (device, nnz entries).
+void level_weights_f64(const GraphView &g, double *out, cudaStream_t s);
 // Dense order-preserving relabel; returns n'.
 uint32_t relabel_dense(const uint32_t *C, uint32_t n, uint32_t *C_dense, CoarsenWorkspace &ws, cudaStream_t s);
 // Next level from a graph and a dense assignment with n' communities.

@@ -325,6 +325,7 @@ void graph_from_device_csr(mg_graph *g, uint32_t n, uint64_t nnz, const uint32_t
 }
 
 void graph_from_level(mg_graph *g, LevelGraph &lv, int integral, double mass) {
+    MG_CHECK(lv.wk == WK_F64, MG_ERR_INVALID, "graph_from_level: f64 level expected");
     cudaStream_t s = g->ctx->stream;
     g->n = lv.n;
     g->nnz = lv.nnz;

@@ -111,6 +111,7 @@ __device__ __forceinline__ void put_sin(const LMArgs &A, uint32_t i, double &sin
 template <int WK>
 __device__ __forceinline__ double wload(const void *w, uint32_t e) {
     if constexpr (WK == WK_UNIT) return 1.0;
+    else if constexpr (WK == WK_U32) return u2d(__ldcs((const uint32_t *)w + e));
     else if constexpr (WK == WK_F32 || WK == WK_F32I) return (double)__ldcs((const float *)w + e);
     else return __ldcs((const double *)w + e);
 }
@@ -371,6 +372,7 @@ __device__ __forceinline__ int table_bits(uint32_t d, int max_bits) {
 template <int WK>
 __device__ __forceinline__ typename ValT<WK>::type wget(const void *w, uint32_t e) {
     if constexpr (WK == WK_UNIT) return 1u;
+    else if constexpr (WK == WK_U32) return __ldcs((const uint32_t *)w + e);
     else if constexpr (WK == WK_F64I)
         return (uint32_t)__double2loint(__dadd_rn(__ldcs((const double *)w + e), 4503599627370496.0));
     else if constexpr (WK == WK_F32I) return __float2uint_rn(__ldcs((const float *)w + e));
@@ -1214,14 +1216,17 @@ void dispatch_kind(const GraphView &g, const SweepParams &p, F &f) {
     MG_SWEEP_CASE(WK_UNIT, MG_PREC_FP64)
     MG_SWEEP_CASE(WK_F32I, MG_PREC_FP64)
     MG_SWEEP_CASE(WK_F64I, MG_PREC_FP64)
+    MG_SWEEP_CASE(WK_U32, MG_PREC_FP64)
     MG_SWEEP_CASE(WK_F32, MG_PREC_FP64)
     MG_SWEEP_CASE(WK_F64, MG_PREC_FP64)
     MG_SWEEP_CASE(WK_UNIT, MG_PREC_INT64)
     MG_SWEEP_CASE(WK_F32I, MG_PREC_INT64)
     MG_SWEEP_CASE(WK_F64I, MG_PREC_INT64)
+    MG_SWEEP_CASE(WK_U32, MG_PREC_INT64)
     MG_SWEEP_CASE(WK_UNIT, MG_PREC_FP32)
     MG_SWEEP_CASE(WK_F32I, MG_PREC_FP32)
     MG_SWEEP_CASE(WK_F64I, MG_PREC_FP32)
+    MG_SWEEP_CASE(WK_U32, MG_PREC_FP32)
     MG_SWEEP_CASE(WK_F32, MG_PREC_FP32)
     MG_SWEEP_CASE(WK_F64, MG_PREC_FP32)
 #undef MG_SWEEP_CASE

@@ -185,10 +185,13 @@ void move_prepare_level(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, c
     if (ws.max_cluster == 0) ws.max_cluster = probe_max_cluster();
     // classes 13..17 are the cluster tiers of 1..16 CTAs (a tier of 2^t CTAs
     // holds degrees up to 2^t * kClusterSlots / 2), class 18 the giants; on a
-    // device without 16-CTA clusters class 17 joins the giants
-    for (int t = 0; t < kTiers; t++) lvl.tier_off[t] = lvl.bins.offset[kFirstHeavyClass + t] - h0;
+    // device without 16-CTA clusters class 17 joins the giants, and so do the
+    // classes from ws.giant_class on
+    int first_giant = std::min(ws.giant_class - kFirstHeavyClass, kTiers - 1);
+    if (ws.max_cluster < 16) first_giant = std::min(first_giant, kTiers - 2);
+    for (int t = 0; t < kTiers; t++)
+        lvl.tier_off[t] = lvl.bins.offset[kFirstHeavyClass + std::min(t, first_giant)] - h0;
     lvl.tier_off[kTiers] = lvl.heavy;
-    if (ws.max_cluster < 16) lvl.tier_off[kTiers - 1] = lvl.tier_off[kTiers - 2];
     lvl.giants = lvl.tier_off[kTiers] - lvl.tier_off[kTiers - 1];
     if (lvl.giants == 0) return;
     const uint32_t H = lvl.giants;
@@ -295,6 +298,7 @@ void level_init(const GraphView &g, double *k, double *sigma, uint32_t *C, cudaS
     unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(g.n, 8), 148ull * 16);
     if (g.wk == WK_UNIT) level_init_kernel<WK_UNIT><<<grid, 256, 0, s>>>(g.off, g.w, g.n, k, sigma, C);
     else if (g.wk == WK_F32) level_init_kernel<WK_F32><<<grid, 256, 0, s>>>(g.off, g.w, g.n, k, sigma, C);
+    else if (g.wk == WK_U32) level_init_kernel<WK_U32><<<grid, 256, 0, s>>>(g.off, g.w, g.n, k, sigma, C);
     else level_init_kernel<WK_F64><<<grid, 256, 0, s>>>(g.off, g.w, g.n, k, sigma, C);
     MG_LAUNCH_CHECK();
 }

@@ -76,6 +76,11 @@ void keep_level_csr(const GraphView &cur, mg_result &res, cudaStream_t s) {
         MG_CUDA(cudaMemcpyAsync(w32.data(), cur.w, sizeof(float) * cur.nnz, cudaMemcpyDeviceToHost, s));
         MG_CUDA(cudaStreamSynchronize(s));
         for (uint64_t e = 0; e < cur.nnz; e++) L.w[e] = w32[e];
+    } else if (cur.nnz && cur.wk == WK_U32) {
+        std::vector<uint32_t> wi(cur.nnz);
+        MG_CUDA(cudaMemcpyAsync(wi.data(), cur.w, sizeof(uint32_t) * cur.nnz, cudaMemcpyDeviceToHost, s));
+        MG_CUDA(cudaStreamSynchronize(s));
+        for (uint64_t e = 0; e < cur.nnz; e++) L.w[e] = wi[e];
     }
 }
 
@@ -133,7 +138,7 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
         int base = 0, pend = 1;
         // first sweep: P = identity (base), proposes C[1]; yields Q0
         sp.up = 1;
-        sp.agg = 0;
+        sp.agg = sweep_agg(ctx->mws, 0);
         // shapes of the light classes (autotuner; its timing runs write the
         // proposal this sweep writes)
         move_tune(cur, mlv, ctx->mws, sp, C[base], C[pend], k, sigma, s);
@@ -161,7 +166,7 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
             sp.up = !sp.up;
             // combine equal communities in the warp once they repeat: fewer
             // than half of the last sweep's edges were distinct candidates
-            sp.agg = 2 * hacc.distinct < cur.nnz;
+            sp.agg = sweep_agg(ctx->mws, 2 * hacc.distinct < cur.nnz);
             const int next = 3 - base - pend;
             Timer ti(ctx->ev[0], ctx->ev[1], s);
             sweep_reset_acc(ctx->mws, s);

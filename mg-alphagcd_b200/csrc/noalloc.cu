@@ -6,8 +6,10 @@
 // a graph they already hold in device memory.  The per-block hash tables,
 // which every other sweep path takes from engine-owned allocations, live
 // here in a fixed file-scope device array of kNoAllocScratchBytes.  Each
-// block processes vertices in turn with its own slice of that array as an
-// open-addressing table of pow2(2 * max degree) slots.  The arithmetic is the
+// block processes vertices in turn with its own slice of that array (room for
+// pow2(2 * max degree + 2) slots); a vertex uses only the first
+// pow2(2 * its degree + 2) slots of it as an open-addressing table, so the
+// work per vertex follows its own degree, not the graph's maximum.  The arithmetic is the
 // engine's FP64 gain (same tie-break, same version 1 / 2 rules), so for
 // integral weights the result equals mg_local_move exactly.
 #include <algorithm>
@@ -72,23 +74,29 @@ __global__ void __launch_bounds__(kNoAllocThreads) noalloc_move_kernel(NoAllocAr
         const uint32_t src = A.C[v];
         const double ki = A.k[v];
         const double a = A.sigma[src] - ki;
+        const uint32_t lo = A.off[v], hi = A.off[v + 1];
+        // this vertex's table: the first ts slots of the block's slice, a
+        // power of two >= 2 * degree + 2 (load <= 1/2); every slot it touches
+        // lies below ts and is cleaned by its evaluation loop
+        uint32_t ts = 32;
+        while (ts < 2 * (hi - lo) + 2 && ts < tsize) ts <<= 1;
         double e_part = 0;
-        for (uint32_t e = A.off[v] + threadIdx.x; e < A.off[v + 1]; e += kNoAllocThreads) {
+        for (uint32_t e = lo + threadIdx.x; e < hi; e += kNoAllocThreads) {
             const uint32_t j = A.col[e];
             const uint32_t c = A.C[j];
             const double w = A.w ? A.w[e] : 1.0;
             if (c != src) {
                 const bool cand = A.version == 1 ? (A.up ? c < src : c > src) : true;
                 if (!cand) continue;
-                uint32_t s = hash_range(c, tsize);
-                for (uint32_t p = 0; p < tsize; p++) {
+                uint32_t s = hash_range(c, ts);
+                for (uint32_t p = 0; p < ts; p++) {
                     uint32_t cur = ((volatile uint32_t *)keys)[s];
                     if (cur == c) break;
                     if (cur == kEmpty) {
                         uint32_t prev = atomicCAS(keys + s, kEmpty, c);
                         if (prev == kEmpty || prev == c) break;
                     }
-                    s = s + 1 == tsize ? 0 : s + 1;
+                    s = s + 1 == ts ? 0 : s + 1;
                 }
                 atomicAdd(vals + s, w);
             } else if (j != v) {
@@ -102,7 +110,7 @@ __global__ void __launch_bounds__(kNoAllocThreads) noalloc_move_kernel(NoAllocAr
         for (int i = 0; i < kNoAllocThreads / 32; i++) e_src += red_e[i];
         double best = 0.0;
         uint32_t dst = src;
-        for (uint32_t s = threadIdx.x; s < tsize; s += kNoAllocThreads) {
+        for (uint32_t s = threadIdx.x; s < ts; s += kNoAllocThreads) {
             const uint32_t c = keys[s];
             if (c == kEmpty) continue;
             const double kic = vals[s];
@@ -159,7 +167,8 @@ extern "C" mg_status mg_local_move_noalloc(uint32_t n, const uint32_t *d_offsets
                                            const double *d_weights, double mass, const uint32_t *d_C,
                                            const double *d_sigma, const double *d_k, uint32_t *d_C_new,
                                            int version, int up, void *stream) {
-    if (!d_offsets || !d_C || !d_sigma || !d_k || !d_C_new) return noalloc_fail(MG_ERR_INVALID, "NULL argument");
+    if (!d_offsets || !d_cols || !d_C || !d_sigma || !d_k || !d_C_new)
+        return noalloc_fail(MG_ERR_INVALID, "NULL argument");
     if (version < 0 || version > 2) return noalloc_fail(MG_ERR_INVALID, "version must be 0, 1 or 2");
     if (n == 0) return MG_OK;
     if (!(mass > 0)) return noalloc_fail(MG_ERR_INVALID, "mass must be positive");

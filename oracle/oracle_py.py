@@ -143,6 +143,10 @@ def set_threads(n: int) -> int:
     return lib().or_set_threads(int(n))
 
 
+def get_threads() -> int:
+    return int(lib().or_get_threads())
+
+
 def mix64(x: int) -> int:
     return int(lib().or_mix64(x & 0xFFFFFFFFFFFFFFFF))
 

@@ -27,13 +27,15 @@ def test_reference_arm_line():
     assert d["value"] > 0 and d["higher_is_better"] is True
     assert d["e2e"]["value"] == d["value"] and d["e2e"]["h2d_bytes_per_step"] == 0
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    # time to solution: one oracle run to convergence beside the sweep samples
+    full = d["full_run"]
+    assert full["seconds"] > 0 and full["iterations"] > 0 and full["levels"][0] == d["config"]["vertices"]
+    assert d["modularity"] == full["modularity"] and d["convergence_s"] == full["seconds"]
     sys.path.insert(0, ROOT)
     import bench
 
-    # the engine arm reports the same workload description
-    cfg = bench.rmat_config(14, d["config"]["vertices"], d["config"]["directed_entries"], "single GPU")
-    assert {k: v for k, v in d["config"].items() if k != "parallelism"} == \
-        {k: v for k, v in cfg.items() if k != "parallelism"}
+    # the engine arm reports the identical workload description
+    assert d["config"] == bench.rmat_config(14, d["config"]["vertices"], d["config"]["directed_entries"])
 
 
 def test_reference_arm_other_ranks_print_nothing():

@@ -5,7 +5,9 @@ static 16 MiB device array instead of engine allocations.
 
 The test gives it device buffers it did not allocate itself (torch tensors),
 calls it through the C ABI twice in a row, and checks each result against
-the regular entry point mg_local_move (bit-exact: integral weights).  It
+the regular entry point mg_local_move and against the oracle (bit-exact:
+integral weights).  One graph has a hub of degree 100,000 among 100,000
+low-degree vertices: each vertex's table follows its own degree.  It
 also checks that a graph whose maximum degree exceeds the static array is
 refused with a clear error.  This file is collected last on purpose.
 """
@@ -38,7 +40,11 @@ def test_noalloc_matches_local_move(O, mg, ctx):
     row = np.repeat(np.arange(base.n), np.diff(base.offsets).astype(np.int64))
     m = row < base.cols
     w = np.random.default_rng(4).integers(1, 6, m.sum()).astype(np.float64)
-    for g in (base, O.csr_from_pairs(base.n, row[m], base.cols[m], w)):
+    leaves = 100_000
+    ring = np.arange(1, leaves + 1)
+    hub = O.csr_from_pairs(leaves + 1, np.concatenate([np.zeros(leaves, np.int64), ring]),
+                           np.concatenate([ring, ring % leaves + 1]))
+    for g in (base, O.csr_from_pairs(base.n, row[m], base.cols[m], w), hub):
         n = g.n
         k = O.vertex_weights(g)
         mass = O.mass(g)
@@ -62,6 +68,8 @@ def test_noalloc_matches_local_move(O, mg, ctx):
                 got = d_out.cpu().numpy().view(np.uint32)
                 want, _ = dg.local_move(C, sig, k, version, up)
                 assert (got == want).all(), (call, version, up, np.nonzero(got != want)[0][:10])
+                ref, _ = O.local_move(g, C, sig, k, mass, version, up)
+                assert (got == ref).all(), (call, version, up, np.nonzero(got != ref)[0][:10])
             C, _ = O.local_move(g, C, sig, k, mass, 2, True)
             sig = np.zeros(n)
             np.add.at(sig, C, k)
