@@ -640,7 +640,7 @@ mg_status mg_tune_load(mg_ctx *ctx, const char *path) {
         char name[16];
         double us;
         if (sscanf(line, "%u %u %u %u %u %u %15s %lf", &wk, &prec, &ver, &bt, &cls, &bucket, name, &us) != 8 ||
-            wk > 4 || prec > 2 || ver > 2 || bt > 1 || cls >= (unsigned)kLightClasses || bucket > 31) {
+            wk > 5 || prec > 2 || ver > 2 || bt > 1 || cls >= (unsigned)kLightClasses || bucket > 31) {
             st = MG_ERR_FORMAT;
             break;
         }

@@ -1,6 +1,7 @@
 // engine.cuh -- internal interfaces between the engine's translation units.
 #pragma once
 
+#include <cstdlib>
 #include <map>
 #include <vector>
 
@@ -65,6 +66,7 @@ constexpr int kTiers = 6;
 enum SweepShape : uint8_t {
     SH_T2, SH_T4, SH_T8, SH_T16, SH_T32,  // tiles
     SH_H32, SH_H64, SH_H128, SH_H256, SH_H512,  // hash, GT threads per vertex
+    SH_W,  // a warp per batch of vertices, a table per vertex (classes 5-10)
     SH_COUNT
 };
 // largest degree a shape serves
@@ -77,6 +79,7 @@ inline uint32_t shape_capacity(int sh) {
         case SH_T32: return 32;
         case SH_H32: return 512;
         case SH_H64: return 1024;
+        case SH_W: return 1024;
         default: return 4096;
     }
 }
@@ -108,6 +111,8 @@ struct TuneEntry {
 };
 struct TuneTable {
     int mode = MG_TUNE_ON;
+    // print every timed candidate to stderr (environment variable MG_TUNE_LOG=1)
+    bool log = getenv("MG_TUNE_LOG") != nullptr && getenv("MG_TUNE_LOG")[0] == '1';
     std::map<uint32_t, TuneEntry> entries;
     unsigned long long tuned = 0;  // classes tuned (timed) so far
     static uint32_t key(int wk, int prec, int ver, int bt, int cls, uint32_t size) {

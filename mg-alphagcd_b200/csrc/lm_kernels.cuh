@@ -619,6 +619,248 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
 }
 
 // ============================================================================
+// classes 5-10: a warp works a batch of K vertices at once (K * D <= 256,
+// D = 2^logd the class's largest degree), each vertex with its own table of
+// 2D slots in the warp's slice of shared memory.  Batch position f = r * 256
+// + p * 32 + lane (round r, step p) is edge f mod D of vertex f / D, so one
+// step belongs to one vertex (D >= 32) and every lane has kWarpP edges -- and
+// later kWarpP candidates -- in flight at once.  Warp-level synchronisation
+// only: no block barrier, no table shared between warps.
+// ============================================================================
+constexpr int kWarpP = 8;                  // entries per lane per round
+constexpr int kWarpF = 32 * kWarpP;        // batch entries per round
+constexpr int kWarpThreads = 256;
+constexpr int kWarpMaxLogD = 10;           // classes up to 10 (degree <= 1024)
+
+// slots of a warp's slice for classes of largest degree 2^logd
+__host__ __device__ constexpr uint32_t warp_slots(int logd) {
+    return 2u * ((1u << logd) > (uint32_t)kWarpF ? (1u << logd) : (uint32_t)kWarpF);
+}
+// bytes of a warp's slice: values V | keys u32 | candidate lists u16 (half
+// the slots) | counters u32[16] | internal and self weights V[8] each
+template <int WK>
+__host__ __device__ constexpr size_t warp_slice_bytes(int logd) {
+    return ((size_t)warp_slots(logd) * (sizeof(typename ValT<WK>::type) + sizeof(uint32_t) + sizeof(uint16_t) / 2) +
+            3 * 8 * 8 + 15) & ~(size_t)15;
+}
+
+template <int WK, int PREC, int VER, int BT>
+__global__ void __launch_bounds__(kWarpThreads) lm_warp_kernel(LMArgs A, uint32_t bin_off, uint32_t bin_size,
+                                                                int logd) {
+    using G = typename Prec<PREC>::G;
+    using V = typename ValT<WK>::type;
+    const int up = load_up<BT>(A);
+    const uint32_t D = 1u << logd;
+    const uint32_t K = D >= (uint32_t)kWarpF ? 1u : (uint32_t)kWarpF / D;  // vertices per batch (<= 8)
+    const uint32_t rounds = D >= (uint32_t)kWarpF ? D / kWarpF : 1u;
+    const uint32_t TS = 2 * D;  // slots per vertex table
+    const int tb = logd + 1;
+    const uint32_t WS = K * TS;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    unsigned char *slice = smem_raw + warp * warp_slice_bytes<WK>(logd);
+    V *vals = (V *)slice;
+    uint32_t *keys = (uint32_t *)(slice + sizeof(V) * WS);
+    uint16_t *used = (uint16_t *)(slice + (sizeof(V) + sizeof(uint32_t)) * WS);
+    uint32_t *cnt = (uint32_t *)(slice + (sizeof(V) + sizeof(uint32_t) + sizeof(uint16_t) / 2) * WS);
+    V *acc_e = (V *)(cnt + 16), *acc_s = acc_e + 8;
+    for (uint32_t s = lane; s < WS; s += 32) {
+        keys[s] = kEmpty;
+        vals[s] = V(0);
+    }
+    if (lane < 8) {
+        cnt[lane] = 0;
+        acc_e[lane] = V(0);
+        acc_s[lane] = V(0);
+    }
+    __syncwarp();
+    double sin = 0;
+    unsigned dcnt = 0;
+    const uint32_t gwarp = blockIdx.x * (kWarpThreads / 32) + warp;
+    const uint32_t nwarp = gridDim.x * (kWarpThreads / 32);
+    for (uint32_t b0 = gwarp * K; b0 < bin_size; b0 += nwarp * K) {  // warp-uniform
+        // lane k < K holds vertex k of the batch
+        uint32_t i = 0, lo = 0, hi = 0, src = kEmpty;
+        double ki = 0;
+        bool act = false;
+        VView vv;
+        vv.P = A.P;
+        vv.N = A.N;
+        if (lane < K && b0 + lane < bin_size) {
+            const uint32_t pos = bin_off + b0 + lane;
+            i = A.perm[pos];
+            if constexpr (BT == 0) {
+                const uint2 r = A.rows[pos];
+                lo = r.x;
+                hi = r.y;
+            }
+            act = vview_at<BT>(A, pos, vv);
+            if (act) {
+                if constexpr (BT != 0) {
+                    lo = A.off[i];
+                    hi = A.off[i + 1];
+                }
+                src = vv.P[i];
+                ki = A.k[i];
+            } else {
+                hi = lo;
+            }
+        }
+        // ---- edge pass: neighbour communities into the vertices' tables ----
+        V e_part = V(0), s_part = V(0);
+        for (uint32_t r = 0; r < rounds; r++) {
+            uint32_t jj[kWarpP], cc[kWarpP];
+            V ww[kWarpP];
+#pragma unroll
+            for (int p = 0; p < kWarpP; p++) {
+                const uint32_t f = r * kWarpF + p * 32 + lane;
+                const uint32_t k = f >> logd;  // uniform over the step
+                const uint32_t lk = __shfl_sync(0xffffffffu, lo, k), hk = __shfl_sync(0xffffffffu, hi, k);
+                const uint32_t e = lk + (f & (D - 1));
+                jj[p] = e < hk ? __ldcs(A.col + e) : kEmpty;
+                ww[p] = e < hk ? wget<WK>(A.w, e) : V(0);
+            }
+#pragma unroll
+            for (int p = 0; p < kWarpP; p++) {
+                const uint32_t k = (r * kWarpF + p * 32) >> logd;
+                const uint32_t *Pk;
+                if constexpr (BT == 0) Pk = A.P;
+                else Pk = (const uint32_t *)__shfl_sync(0xffffffffu, (unsigned long long)vv.P, k);
+                cc[p] = jj[p] != kEmpty ? Pk[jj[p]] : kEmpty;
+            }
+#pragma unroll
+            for (int p = 0; p < kWarpP; p++) {
+                const uint32_t f0 = r * kWarpF + p * 32;
+                const uint32_t k = f0 >> logd;
+                const uint32_t sk = __shfl_sync(0xffffffffu, src, k);
+                const uint32_t ik = __shfl_sync(0xffffffffu, i, k);
+                const uint32_t c = cc[p];
+                uint32_t hnew = kEmpty;
+                if (jj[p] != kEmpty) {
+                    if (c != sk) {
+                        if (is_candidate<VER>(c, sk, up)) {
+                            uint32_t *tk = keys + k * TS;
+                            uint32_t h = hash_slot(c, tb);
+                            for (uint32_t q = 0; q < TS; q++) {
+                                const uint32_t cur = ((volatile uint32_t *)tk)[h];
+                                if (cur == c) break;
+                                if (cur == kEmpty) {
+                                    const uint32_t prev = atomicCAS(tk + h, kEmpty, c);
+                                    if (prev == kEmpty) {
+                                        hnew = h;
+                                        break;
+                                    }
+                                    if (prev == c) break;
+                                }
+                                h = (h + 1) & (TS - 1);
+                            }
+                            atomicAdd(vals + k * TS + h, ww[p]);
+                        }
+                    } else if (jj[p] != ik) {
+                        e_part += ww[p];
+                    } else {
+                        s_part += ww[p];
+                    }
+                }
+                // the step's new slots join vertex k's candidate list
+                const uint32_t m = __ballot_sync(0xffffffffu, hnew != kEmpty);
+                if (m) {
+                    uint32_t pos = 0;
+                    if (lane == 0) {
+                        pos = cnt[k];
+                        cnt[k] = pos + __popc(m);
+                    }
+                    pos = __shfl_sync(0xffffffffu, pos, 0);
+                    if (hnew != kEmpty) used[k * D + pos + __popc(m & ((1u << lane) - 1u))] = (uint16_t)hnew;
+                }
+                // last step of vertex k: its internal and self weight
+                if (((f0 + 32) & (D - 1)) == 0) {
+                    const V te = warp_sum(e_part), ts = warp_sum(s_part);
+                    if (lane == 0) {
+                        acc_e[k] += te;
+                        acc_s[k] += ts;
+                    }
+                    e_part = V(0);
+                    s_part = V(0);
+                }
+            }
+        }
+        __syncwarp();
+        // sigma of the vertex's own community, loaded after the edge pass
+        const double a = act ? A.sigma[src] - ki : 0.0;
+        // ---- candidate pass: score every distinct candidate, argmax per vertex ----
+        G best = G(0);
+        uint32_t dst = 0;
+        for (uint32_t r = 0; r < rounds; r++) {
+            uint32_t kk[kWarpP];
+            double kv[kWarpP], sc[kWarpP];
+#pragma unroll
+            for (int p = 0; p < kWarpP; p++) {
+                const uint32_t f = r * kWarpF + p * 32 + lane;
+                const uint32_t k = f >> logd, u = f & (D - 1);
+                kk[p] = kEmpty;
+                if (u < cnt[k]) {
+                    const uint32_t h = k * TS + used[k * D + u];
+                    kk[p] = keys[h];
+                    kv[p] = v2d(vals[h]);
+                    keys[h] = kEmpty;
+                    vals[h] = V(0);
+                }
+            }
+#pragma unroll
+            for (int p = 0; p < kWarpP; p++)
+                if (kk[p] != kEmpty) sc[p] = A.sigma[kk[p]];
+#pragma unroll
+            for (int p = 0; p < kWarpP; p++) {
+                const uint32_t f0 = r * kWarpF + p * 32;
+                const uint32_t k = f0 >> logd;
+                if ((f0 & (D - 1)) == 0) {  // first step of vertex k
+                    best = G(0);
+                    dst = __shfl_sync(0xffffffffu, src, k);
+                }
+                const double kik = __shfl_sync(0xffffffffu, ki, k);
+                const double ak = __shfl_sync(0xffffffffu, a, k);
+                if (kk[p] != kEmpty) {
+                    const double ek = v2d(acc_e[k]);
+                    GainK Kk;
+                    if constexpr (BT == 0) Kk = A.K;
+                    else Kk = A.gk[A.pgid[bin_off + b0 + k]];
+                    const G gn = Prec<PREC>::gain(kv[p], ek, kik, ak, sc[p], Kk);
+                    if (better(gn, kk[p], best, dst, up)) {
+                        best = gn;
+                        dst = kk[p];
+                    }
+                }
+                if (((f0 + 32) & (D - 1)) == 0) {  // last step of vertex k: argmax, result
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        const G g2 = shfl_xor_g(best, o);
+                        const uint32_t c2 = __shfl_xor_sync(0xffffffffu, dst, o);
+                        if (better(g2, c2, best, dst, up)) {
+                            best = g2;
+                            dst = c2;
+                        }
+                    }
+                    if (lane == k && act) {
+                        vv.N[i] = final_choice<VER>(dst, src, up);
+                        put_sin<BT>(A, i, sin, v2d(acc_e[k]) + v2d(acc_s[k]));
+                        dcnt += cnt[k];
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        if (lane < K) {
+            cnt[lane] = 0;
+            acc_e[lane] = V(0);
+            acc_s[lane] = V(0);
+        }
+        __syncwarp();
+    }
+    flush_acc(A.acc, A.integral, sin, dcnt);
+}
+
+// ============================================================================
 // classes 13-17: one vertex per thread-block cluster of CS CTAs, the
 // cluster's shared memory holding one hash table of CS * kClusterSlots slots.
 // A neighbour community hashes to (owner CTA, slot); the owner's segment
@@ -1136,6 +1378,15 @@ void launch_light(int shape, int cls, const LMArgs &A, uint32_t off, uint32_t si
         kern<<<grid, block, smem, s>>>(A, off, size, sl);
         MG_LAUNCH_CHECK();
     };
+    auto warpk = [&](auto kern) {
+        const int logd = std::max(5, cls);
+        const size_t smem = (kWarpThreads / 32) * warp_slice_bytes<WK>(logd);
+        raise_smem_limit((const void *)kern, (kWarpThreads / 32) * warp_slice_bytes<WK>(kWarpMaxLogD));
+        const uint32_t K = (1u << logd) >= (uint32_t)kWarpF ? 1u : (uint32_t)kWarpF >> logd;
+        const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(size, (kWarpThreads / 32) * K), 148ull * 8);
+        kern<<<grid, kWarpThreads, smem, s>>>(A, off, size, logd);
+        MG_LAUNCH_CHECK();
+    };
     switch (shape) {
         case SH_T2: tile(lm_tile_kernel<2, WK, PREC, VER, BT>, 2); break;
         case SH_T4: tile(lm_tile_kernel<4, WK, PREC, VER, BT>, 4); break;
@@ -1147,6 +1398,7 @@ void launch_light(int shape, int cls, const LMArgs &A, uint32_t off, uint32_t si
         case SH_H128: hash(lm_hash_kernel<128, WK, PREC, VER, 128, BT>, 128, 128); break;
         case SH_H256: hash(lm_hash_kernel<256, WK, PREC, VER, 256, BT>, 256, 256); break;
         case SH_H512: hash(lm_hash_kernel<512, WK, PREC, VER, 512, BT>, 512, 512); break;
+        case SH_W: warpk(lm_warp_kernel<WK, PREC, VER, BT>); break;
         default: throw Error(MG_ERR_INVALID, "unknown sweep shape");
     }
 }
@@ -1284,15 +1536,17 @@ inline std::vector<int> tune_candidates(int cls) {
         out.push_back(t0);
         if (t0 < SH_T32) out.push_back(t0 + 1);
         out.push_back(SH_H32);
+        if (cls == 5) out.push_back(SH_W);
         return out;
     }
+    if (shape_capacity(SH_W) >= maxdeg) out.push_back(SH_W);
     for (int sh = SH_H32; sh <= SH_H512; sh++) {
         if (shape_capacity(sh) < maxdeg) continue;
         // wider groups than twice the degree leave most threads idle
         const uint32_t gt = 32u << (sh - SH_H32);
         if (gt > 2 * maxdeg && sh > SH_H32) continue;
         out.push_back(sh);
-        if (out.size() == 3) break;
+        if (out.size() == 4) break;
     }
     return out;
 }
@@ -1330,6 +1584,8 @@ void tune_light(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, const Swe
                 MG_CUDA(cudaEventSynchronize(e1));
                 MG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
             }
+            if (T.log) fprintf(stderr, "tune: wk %d prec %d ver %d batched %d class %d size %u shape %s %.1f us\n", wk,
+                               p.precision, p.version, BT, c, size, shape_name(sh), ms * 1000.0);
             if (ms < best) {
                 best = ms;
                 best_sh = sh;

@@ -132,7 +132,7 @@ int probe_max_cluster() {
 }  // namespace
 
 const char *shape_name(int sh) {
-    static const char *names[SH_COUNT] = {"t2", "t4", "t8", "t16", "t32", "h32", "h64", "h128", "h256", "h512"};
+    static const char *names[SH_COUNT] = {"t2", "t4", "t8", "t16", "t32", "h32", "h64", "h128", "h256", "h512", "w"};
     return sh >= 0 && sh < SH_COUNT ? names[sh] : "?";
 }
 
