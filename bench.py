@@ -213,6 +213,20 @@ def traffic_per_sweep():
         return None, None
 
 
+def pinned_csr(g):
+    """The graph's CSR (offsets u64, cols u32) copied into page-locked host
+    memory, as a caller that streams graphs to the GPU would hold it."""
+    import numpy as np
+    import torch
+
+    off_d, cols_d, _ = g.csr()
+    off = torch.empty(len(off_d), dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+    cols = torch.empty(len(cols_d), dtype=torch.int32).pin_memory().numpy().view(np.uint32)
+    off[:] = off_d
+    cols[:] = cols_d
+    return off, cols
+
+
 def cpu_baseline_sample(csr, threads):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py as O
@@ -573,9 +587,9 @@ def run_engine(args, world, rank, local, pg):
     peak, peak_kind = peaks()
     traffic, traffic_alg = traffic_per_sweep()
 
-    # end to end through the public API with host buffers: upload the CSR,
-    # run, read the assignment back
-    off, cols, _ = g.csr()
+    # end to end through the public API with host buffers: upload the CSR
+    # from pinned host memory, run, read the assignment back
+    off, cols = pinned_csr(g)
     e2e_t, e2e_e = 0.0, 0
     for i in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
         t0 = time.perf_counter()

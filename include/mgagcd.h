@@ -287,12 +287,33 @@ enum {
     MG_FILL_OWN = 1,   /* every CTA of a cluster reads the whole row and inserts the communities it owns */
     MG_FILL_SPLIT = 2  /* the CTAs split the row; equal communities combined in the warp; inserts via DSMEM */
 };
+/* Coarsening (coarsen_graph_mg::coarsen_graph, src/coarsen_graph/coarsen_graph_mg.cu:2054-2240)
+ * turns every edge into a (community, neighbour community) key and sorts the
+ * keys; with combining, the 32 edges a warp holds are first merged by key, so
+ * the sort sees far fewer keys where communities repeat inside rows.  The
+ * next-level graph is the same either way. */
+enum {
+    MG_COMBINE_AUTO = 0, /* in a run: combine when the phase's last sweep saw few distinct candidates; mg_coarsen: off */
+    MG_COMBINE_OFF = 1,
+    MG_COMBINE_ON = 2
+};
 typedef struct {
-    int cluster_fill; /* MG_FILL_* */
-    int giant_class;  /* degree classes >= this (13..18) take the global-table path; 0 = default (18) */
+    int cluster_fill;    /* MG_FILL_* */
+    int giant_class;     /* degree classes >= this (13..18) take the global-table path; 0 = default (18) */
+    int coarsen_combine; /* MG_COMBINE_* */
 } mg_sweep_opts;
 /* Set the context's policy (opts NULL = defaults); applies to later sweeps and runs. */
 mg_status mg_sweep_options(mg_ctx *ctx, const mg_sweep_opts *opts);
+
+/* ---- fault injection (test hook) ----------------------------------------------
+ * No reference counterpart (the reference exits on any CUDA error,
+ * include/common.h:53-83).  Arms a process-wide countdown: the nth device
+ * allocation the library makes from now on fails as if cudaMalloc had run out
+ * of memory (once; nth = 0 disarms).  *pending (may be NULL) receives what was
+ * left of the previous countdown (0 = it fired or was never armed).  The
+ * entry point that hits it returns MG_ERR_OOM with text, releases what it
+ * allocated, and the context stays usable.  No GPU fault is involved. */
+mg_status mg_test_fail_allocation(uint64_t nth, uint64_t *pending);
 
 /* ---- batched form --------------------------------------------------------------
  * No reference counterpart: the reference runs one graph per process.  A batch

@@ -49,7 +49,7 @@ class _Opts(ct.Structure):
 
 
 class _SweepOpts(ct.Structure):
-    _fields_ = [("cluster_fill", ct.c_int), ("giant_class", ct.c_int)]
+    _fields_ = [("cluster_fill", ct.c_int), ("giant_class", ct.c_int), ("coarsen_combine", ct.c_int)]
 
 
 class _RunOpts(ct.Structure):
@@ -120,10 +120,11 @@ EXPORTED = [
     "mg_serve_cancel", "mg_serve_release", "mg_serve_stats", "mg_serve_last_error", "mg_serve_stop",
     "mg_tune_mode", "mg_tune_table", "mg_tune_save", "mg_tune_load", "mg_graph_generate_chunglu",
     "mg_graph_from_mtx_ex", "mg_csr_from_mtx", "mg_csr_info", "mg_csr_arrays", "mg_csr_free",
-    "mg_result_level_map", "mg_result_level_csr", "mg_sweep_options",
+    "mg_result_level_map", "mg_result_level_csr", "mg_sweep_options", "mg_test_fail_allocation",
 ]
 TUNE_OFF, TUNE_CACHED, TUNE_ON = 0, 1, 2
 FILL_AUTO, FILL_OWN, FILL_SPLIT = 0, 1, 2
+COMBINE_AUTO, COMBINE_OFF, COMBINE_ON = 0, 1, 2
 LOAD_CACHE_READ, LOAD_CACHE_WRITE = 1, 2
 
 
@@ -187,6 +188,7 @@ def lib():
     L.mg_batch_generate.argtypes = [vp, u32, vp, pp]
     L.mg_tune_mode.argtypes = [vp, i32]
     L.mg_sweep_options.argtypes = [vp, ct.POINTER(_SweepOpts)]
+    L.mg_test_fail_allocation.argtypes = [u64, ct.POINTER(u64)]
     L.mg_tune_table.argtypes = [vp, ct.c_char_p, ct.c_size_t, ct.POINTER(ct.c_size_t)]
     L.mg_tune_save.argtypes = [vp, ct.c_char_p]
     L.mg_tune_load.argtypes = [vp, ct.c_char_p]
@@ -305,11 +307,13 @@ class Context:
         """TUNE_OFF: built-in shapes; TUNE_CACHED: table only; TUNE_ON: also time new classes."""
         self.check(lib().mg_tune_mode(self.h, mode), "mg_tune_mode")
 
-    def sweep_options(self, cluster_fill: int = FILL_AUTO, giant_class: int = 0):
-        """Heavy-vertex policy (mg_sweep_options): the cluster-table fill
-        (FILL_*) and the first degree class (13..18, 0 = default) sent to the
-        global-table path.  Results do not depend on it."""
-        o = _SweepOpts(cluster_fill, giant_class)
+    def sweep_options(self, cluster_fill: int = FILL_AUTO, giant_class: int = 0,
+                      coarsen_combine: int = COMBINE_AUTO):
+        """Sweep and coarsening policy (mg_sweep_options): the cluster-table
+        fill (FILL_*), the first degree class (13..18, 0 = default) sent to
+        the global-table path, and warp combining of equal keys in the
+        coarsening (COMBINE_*).  Results do not depend on it."""
+        o = _SweepOpts(cluster_fill, giant_class, coarsen_combine)
         self.check(lib().mg_sweep_options(self.h, ct.byref(o)), "mg_sweep_options")
 
     def tune_table(self) -> list:
@@ -474,6 +478,15 @@ class Server:
             self.stop()
         except Exception:
             pass
+
+
+def fail_allocation(nth: int) -> int:
+    """Test hook (mg_test_fail_allocation): the nth device allocation of the
+    library from now on fails as out of memory (0 disarms).  Returns what was
+    left of the previous countdown (0: it fired, or was not armed)."""
+    left = ct.c_uint64()
+    lib().mg_test_fail_allocation(nth, ct.byref(left))
+    return int(left.value)
 
 
 def load_mtx(path: str, cache_read: bool = False, cache_write: bool = False) -> dict:

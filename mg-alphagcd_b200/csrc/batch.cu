@@ -727,7 +727,8 @@ void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &re
             std::swap(goff, goff_new);  // the assignment is in the relabelled ids
             break;
         }
-        coarsen_level(cur, Cd, nn, integral, ctx->lv[lvl_out], ctx->cws, s, nullptr);
+        coarsen_level(cur, Cd, nn, integral, ctx->lv[lvl_out], ctx->cws, s, nullptr,
+                      ctx->mws.coarsen_combine == MG_COMBINE_ON);
         MG_CUDA(cudaEventRecord(ctx->ev[1], s));
         MG_CUDA(cudaEventSynchronize(ctx->ev[1]));
         MG_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));

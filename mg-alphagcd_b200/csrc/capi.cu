@@ -1,6 +1,7 @@
 // capi.cu -- the extern "C" entry points declared in include/mgagcd.h.
 // Every entry point catches engine errors and returns an mg_status; the
 // message of the last failure is kept on the context.
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -61,6 +62,16 @@ mg_ctx::~mg_ctx() {
 
 namespace mg {
 thread_local unsigned long long g_kernel_launches = 0;
+
+static std::atomic<long long> g_alloc_fault_countdown{0};  // 0: disarmed
+
+bool alloc_fault_due() {
+    long long c = g_alloc_fault_countdown.load(std::memory_order_relaxed);
+    while (c > 0) {
+        if (g_alloc_fault_countdown.compare_exchange_weak(c, c - 1)) return c == 1;
+    }
+    return false;
+}
 
 // error text for entry points that run without a context (mg_last_error(NULL))
 void set_orphan_error(const std::string &msg) { g_orphan_error = msg; }
@@ -455,7 +466,8 @@ mg_status mg_coarsen(mg_graph *g, const uint32_t *C, uint32_t *C_dense, mg_graph
         uint32_t *dCd = ctx->Cd.ensure((size_t)n + 1);
         uint32_t nn = relabel_dense(dC, n, dCd, ctx->cws, s);
         LevelGraph lv;
-        coarsen_level(g->view(), dCd, nn, g->integral, lv, ctx->cws, s, nullptr);
+        coarsen_level(g->view(), dCd, nn, g->integral, lv, ctx->cws, s, nullptr,
+                      ctx->mws.coarsen_combine == MG_COMBINE_ON);
         if (C_dense && n) {
             MG_CUDA(cudaMemcpyAsync(C_dense, dCd, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
         }
@@ -593,15 +605,25 @@ mg_status mg_tune_mode(mg_ctx *ctx, int mode) {
     return MG_OK;
 }
 
+mg_status mg_test_fail_allocation(uint64_t nth, uint64_t *pending) {
+    const long long before = g_alloc_fault_countdown.exchange((long long)nth);
+    if (pending) *pending = before > 0 ? (uint64_t)before : 0;
+    return MG_OK;
+}
+
 mg_status mg_sweep_options(mg_ctx *ctx, const mg_sweep_opts *opts) {
     if (!ctx) return MG_ERR_INVALID;
     const int fill = opts ? opts->cluster_fill : MG_FILL_AUTO;
+    const int comb = opts ? opts->coarsen_combine : MG_COMBINE_AUTO;
+    if (comb < MG_COMBINE_AUTO || comb > MG_COMBINE_ON)
+        return fail(ctx, MG_ERR_INVALID, "mg_sweep_options: unknown coarsen_combine");
     const int gc = opts && opts->giant_class ? opts->giant_class : kFirstHeavyClass + kTiers - 1;
     if (fill < MG_FILL_AUTO || fill > MG_FILL_SPLIT) return fail(ctx, MG_ERR_INVALID, "mg_sweep_options: unknown fill");
     if (gc < kFirstHeavyClass || gc > kFirstHeavyClass + kTiers - 1)
         return fail(ctx, MG_ERR_INVALID, "mg_sweep_options: giant_class must be 0 or 13..18");
     ctx->mws.cluster_fill = fill;
     ctx->mws.giant_class = gc;
+    ctx->mws.coarsen_combine = comb;
     return MG_OK;
 }
 

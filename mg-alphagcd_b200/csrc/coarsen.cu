@@ -37,21 +37,29 @@ __global__ void apply_relabel_kernel(const uint32_t *C, uint32_t n, const uint32
 // the non-empty one, wins), a prefix maximum over the tile then gives every
 // edge its row, and the keys are written with coalesced loads and stores.
 // One binary search per tile finds the row holding its first edge.
+// COMBINE: the 32 edges a warp holds at a time are merged by key first (equal
+// keys add their weights, a unit edge counting 1), and only one entry per
+// distinct key is written, to the tile's own region of the output in
+// arrival order; tcount[tile] receives the tile's entry count.  Pays where
+// communities repeat within rows (the end of a phase whose last sweep saw
+// few distinct neighbour communities): the sort then sees far fewer keys.
 constexpr int kExpandThreads = 256;
 constexpr int kExpandPer = 16;
 constexpr uint32_t kExpandTile = kExpandThreads * kExpandPer;
 
-template <int WK, class PV>
+template <int WK, class PV, bool COMBINE = false>
 __global__ void __launch_bounds__(kExpandThreads) expand_keys_kernel(const uint32_t *off, const uint32_t *col,
                                                                      const void *w, uint32_t n, uint64_t m,
                                                                      const uint32_t *Cd, int bc, uint64_t *keys,
-                                                                     PV *vals) {
+                                                                     PV *vals, uint32_t *tcount = nullptr) {
     // tile position q lives at q + q/32 (one padding word per 32: the
     // per-thread runs of 16 positions then fall on distinct banks)
     __shared__ uint32_t rowat[kExpandTile + kExpandTile / 32];
     __shared__ uint32_t part[kExpandThreads];
-    __shared__ uint32_t r0s;
+    __shared__ uint32_t r0s, tcnt;
+    __shared__ PV wstage[COMBINE ? kExpandThreads : 1];
     const uint32_t t = threadIdx.x;
+    if (COMBINE && t == 0) tcnt = 0;
     for (uint64_t E0 = (uint64_t)blockIdx.x * kExpandTile; E0 < m; E0 += (uint64_t)gridDim.x * kExpandTile) {
         const uint64_t E1 = E0 + kExpandTile < m ? E0 + kExpandTile : m;
         if (t == 0) {
@@ -124,18 +132,81 @@ __global__ void __launch_bounds__(kExpandThreads) expand_keys_kernel(const uint3
             }
         }
         __syncthreads();
+        if constexpr (!COMBINE) {
 #pragma unroll 4
-        for (int k = 0; k < kExpandPer; k++) {
-            const uint32_t q = k * kExpandThreads + t;
-            const uint64_t e = E0 + q;
-            if (e < E1) {
-                keys[e] = ((uint64_t)Cd[rowat[q + (q >> 5)]] << bc) | Cd[__ldcs(col + e)];
-                if constexpr (WK == WK_F32) vals[e] = (PV)__ldcs((const float *)w + e);
-                else if constexpr (WK == WK_F64) vals[e] = (PV)__ldcs((const double *)w + e);
-                else if constexpr (WK == WK_U32) vals[e] = (PV)__ldcs((const uint32_t *)w + e);
+            for (int k = 0; k < kExpandPer; k++) {
+                const uint32_t q = k * kExpandThreads + t;
+                const uint64_t e = E0 + q;
+                if (e < E1) {
+                    keys[e] = ((uint64_t)Cd[rowat[q + (q >> 5)]] << bc) | Cd[__ldcs(col + e)];
+                    if constexpr (WK == WK_F32) vals[e] = (PV)__ldcs((const float *)w + e);
+                    else if constexpr (WK == WK_F64) vals[e] = (PV)__ldcs((const double *)w + e);
+                    else if constexpr (WK == WK_U32) vals[e] = (PV)__ldcs((const uint32_t *)w + e);
+                }
+            }
+        } else {
+            const uint32_t lane = t & 31u;
+            const uint64_t tile_base = E0;  // the tile's region of the output
+#pragma unroll 2
+            for (int k = 0; k < kExpandPer; k++) {
+                const uint32_t q = k * kExpandThreads + t;
+                const uint64_t e = E0 + q;
+                uint64_t key = ~0ull;
+                PV v = PV(0);
+                if (e < E1) {
+                    key = ((uint64_t)Cd[rowat[q + (q >> 5)]] << bc) | Cd[__ldcs(col + e)];
+                    if constexpr (WK == WK_UNIT) v = PV(1);
+                    else if constexpr (WK == WK_F32) v = (PV)__ldcs((const float *)w + e);
+                    else if constexpr (WK == WK_F64) v = (PV)__ldcs((const double *)w + e);
+                    else v = (PV)__ldcs((const uint32_t *)w + e);
+                }
+                const uint32_t peers = __match_any_sync(0xffffffffu, key);
+                const bool lead = key != ~0ull && (uint32_t)(__ffs(peers) - 1) == lane;
+                if constexpr (std::is_same<PV, uint32_t>::value) {
+                    v = __reduce_add_sync(peers, v);
+                } else {
+                    wstage[t] = v;
+                    __syncwarp();
+                    if (lead) {
+                        PV s = PV(0);
+                        for (uint32_t mset = peers; mset; mset &= mset - 1) s += wstage[(t & ~31u) + __ffs(mset) - 1];
+                        v = s;
+                    }
+                    __syncwarp();
+                }
+                const uint32_t lm = __ballot_sync(0xffffffffu, lead);
+                if (lm) {
+                    uint32_t pos = 0;
+                    if (lane == (uint32_t)(__ffs(lm) - 1)) pos = atomicAdd(&tcnt, (uint32_t)__popc(lm));
+                    pos = __shfl_sync(0xffffffffu, pos, __ffs(lm) - 1);
+                    if (lead) {
+                        const uint64_t o = tile_base + pos + __popc(lm & ((1u << lane) - 1u));
+                        keys[o] = key;
+                        vals[o] = v;
+                    }
+                }
+            }
+            __syncthreads();
+            if (t == 0) {
+                tcount[E0 / kExpandTile] = tcnt;
+                tcnt = 0;
             }
         }
-        __syncthreads();  // rowat is reused by the next tile
+        __syncthreads();  // rowat (and the tile counter) are reused by the next tile
+    }
+}
+
+// gather the tiles' combined entries into one dense array
+template <class PV>
+__global__ void compact_tiles_kernel(const uint64_t *keys, const PV *vals, const uint32_t *toff, uint64_t tiles,
+                                     uint64_t *okeys, PV *ovals) {
+    for (uint64_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint32_t a = toff[tile], b = toff[tile + 1];
+        const uint64_t src = tile * kExpandTile;
+        for (uint32_t i = threadIdx.x; i < b - a; i += blockDim.x) {
+            okeys[a + i] = keys[src + i];
+            ovals[a + i] = vals[src + i];
+        }
     }
 }
 
@@ -343,7 +414,7 @@ uint32_t relabel_dense(const uint32_t *C, uint32_t n, uint32_t *C_dense, Coarsen
 }
 
 void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int integral, LevelGraph &out,
-                   CoarsenWorkspace &ws, cudaStream_t s, uint64_t *upper_degree_off) {
+                   CoarsenWorkspace &ws, cudaStream_t s, uint64_t *upper_degree_off, bool combine) {
     const size_t m = g.nnz;
     const int bc = bits_for(n_new);
     if (upper_degree_off) {
@@ -363,9 +434,11 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
         out.wi.ensure(1);
         return;
     }
+    if (g.wk == WK_UNIT && !integral) combine = false;  // (a unit graph is always integral)
     uint64_t *keys = ws.keys.ensure(m);
     uint64_t *keys2 = ws.keys_alt.ensure(m);
-    const bool weighted = g.wk != WK_UNIT;
+    // combined entries carry their summed weight (unit edges count 1)
+    const bool weighted = g.wk != WK_UNIT || combine;
     double *vals = weighted ? ws.vals.ensure(m + 1) : nullptr;
     double *vals2 = weighted ? ws.vals_alt.ensure(m + 1) : nullptr;
     // integral weights travel through the sort as 32-bit integers (exact:
@@ -373,46 +446,74 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
     const bool ipay = weighted && integral;
     uint32_t *ivals = (uint32_t *)vals, *ivals2 = (uint32_t *)vals2;
     // one block per tile, at most 8 resident per SM (grid-stride over tiles)
-    const unsigned gw = grid_for(ceil_div(m, kExpandTile), 1, 148ull * 8);
-    auto expand = [&](auto *pv) {
+    const uint64_t tiles = ceil_div(m, kExpandTile);
+    const unsigned gw = grid_for(tiles, 1, 148ull * 8);
+    uint32_t *tcount = combine ? ws.tcount.ensure(tiles + 1) : nullptr;
+    auto expand = [&](auto *pv, auto comb) {
         using PV = typename std::remove_pointer<decltype(pv)>::type;
+        constexpr bool CB = decltype(comb)::value;
         if (g.wk == WK_UNIT)
-            expand_keys_kernel<WK_UNIT, PV><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
+            expand_keys_kernel<WK_UNIT, PV, CB><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys,
+                                                                               pv, tcount);
         else if (g.wk == WK_F32)
-            expand_keys_kernel<WK_F32, PV><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
+            expand_keys_kernel<WK_F32, PV, CB><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys,
+                                                                              pv, tcount);
         else if (g.wk == WK_U32)
-            expand_keys_kernel<WK_U32, PV><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
-        else expand_keys_kernel<WK_F64, PV><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys, pv);
+            expand_keys_kernel<WK_U32, PV, CB><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys,
+                                                                              pv, tcount);
+        else
+            expand_keys_kernel<WK_F64, PV, CB><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys,
+                                                                              pv, tcount);
         MG_LAUNCH_CHECK();
     };
-    if (ipay) expand(ivals);
-    else expand(vals);
+    // the sort's input: every edge (mm = m), or the combined entries gathered
+    // densely into the alternate buffers (mm = their count)
+    size_t mm = m;
+    if (combine) {
+        if (ipay) expand(ivals, std::true_type());
+        else expand(vals, std::true_type());
+        exclusive_scan<uint32_t>(tcount, tcount, tiles, tcount + tiles, s, ws.prim);
+        uint32_t d = 0;
+        MG_CUDA(cudaMemcpyAsync(&d, tcount + tiles, sizeof d, cudaMemcpyDeviceToHost, s));
+        MG_CUDA(cudaStreamSynchronize(s));
+        const unsigned gc = grid_for(tiles, 1, 148ull * 16);
+        if (ipay) compact_tiles_kernel<uint32_t><<<gc, 256, 0, s>>>(keys, ivals, tcount, tiles, keys2, ivals2);
+        else compact_tiles_kernel<double><<<gc, 256, 0, s>>>(keys, vals, tcount, tiles, keys2, vals2);
+        MG_LAUNCH_CHECK();
+        std::swap(keys, keys2);
+        std::swap(vals, vals2);
+        std::swap(ivals, ivals2);
+        mm = d;
+    } else {
+        if (ipay) expand(ivals, std::false_type());
+        else expand(vals, std::false_type());
+    }
     bool flipped;
-    if (ipay) flipped = radix_sort<uint32_t>(keys, ivals, keys2, ivals2, m, 2 * bc, s, ws.prim);
-    else if (weighted) flipped = radix_sort<double>(keys, vals, keys2, vals2, m, 2 * bc, s, ws.prim);
-    else flipped = radix_sort<NoVal>(keys, (NoVal *)nullptr, keys2, (NoVal *)nullptr, m, 2 * bc, s, ws.prim);
+    if (ipay) flipped = radix_sort<uint32_t>(keys, ivals, keys2, ivals2, mm, 2 * bc, s, ws.prim);
+    else if (weighted) flipped = radix_sort<double>(keys, vals, keys2, vals2, mm, 2 * bc, s, ws.prim);
+    else flipped = radix_sort<NoVal>(keys, (NoVal *)nullptr, keys2, (NoVal *)nullptr, mm, 2 * bc, s, ws.prim);
     const uint64_t *sk = flipped ? keys2 : keys;
     const double *sv = flipped ? vals2 : vals;
     uint32_t *ustart, *seg, *head;
-    uint32_t u = unique_runs(sk, m, bc, n_new, out, ws, s, &ustart, &seg, &head);
+    uint32_t u = unique_runs(sk, mm, bc, n_new, out, ws, s, &ustart, &seg, &head);
     if (integral && !weighted) {
-        run_lengths_kernel<uint32_t><<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)m, out.wi.ensure(u + 1));
+        run_lengths_kernel<uint32_t><<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)mm, out.wi.ensure(u + 1));
         MG_LAUNCH_CHECK();
     } else if (!weighted) {
-        run_lengths_kernel<double><<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)m, out.w.ensure(u + 1));
+        run_lengths_kernel<double><<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)mm, out.w.ensure(u + 1));
         MG_LAUNCH_CHECK();
     } else if (integral) {
         // exact: 64-bit prefix sums over the sorted weights, run sum = difference
         uint64_t *pre = (uint64_t *)(flipped ? vals : vals2);
-        to_u64_kernel<uint32_t><<<grid_for(m), 256, 0, s>>>(flipped ? ivals2 : ivals, m, pre);
+        to_u64_kernel<uint32_t><<<grid_for(mm), 256, 0, s>>>(flipped ? ivals2 : ivals, mm, pre);
         MG_LAUNCH_CHECK();
-        exclusive_scan<uint64_t>(pre, pre, m, pre + m, s, ws.prim);
-        run_diff_kernel<<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)m, pre, out.wi.ensure(u + 1));
+        exclusive_scan<uint64_t>(pre, pre, mm, pre + mm, s, ws.prim);
+        run_diff_kernel<<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)mm, pre, out.wi.ensure(u + 1));
         MG_LAUNCH_CHECK();
     } else {
         double *w = out.w.ensure(u + 1);
         MG_CUDA(cudaMemsetAsync(w, 0, sizeof(double) * u, s));
-        run_sums_kernel<<<(unsigned)ceil_div(ceil_div(m, kSegItems), 256), 256, 0, s>>>(sv, m, seg, head, w);
+        run_sums_kernel<<<(unsigned)ceil_div(ceil_div(mm, kSegItems), 256), 256, 0, s>>>(sv, mm, seg, head, w);
         MG_LAUNCH_CHECK();
     }
 }

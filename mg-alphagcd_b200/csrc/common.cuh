@@ -63,6 +63,11 @@ inline uint32_t pow2_at_least(uint64_t x, uint32_t lo = 16) {
 }
 
 // ---- device buffers ------------------------------------------------------
+// Allocation-failure injection (test hook, mg_test_fail_allocation): when
+// armed with n, the n-th device allocation of the library from then on fails
+// as out of memory, once.  Process-wide.
+bool alloc_fault_due();
+
 // Grow-only device allocation owned by the engine (cudaMalloc on growth only).
 template <class T>
 struct DBuf {
@@ -81,6 +86,7 @@ struct DBuf {
         if (n > cap) {
             release();
             size_t want = n < 16 ? 16 : n;
+            if (alloc_fault_due()) throw Error(MG_ERR_OOM, "device allocation failed (injected by mg_test_fail_allocation)");
             MG_CUDA(cudaMalloc(&p, want * sizeof(T)));
             cap = want;
         }

@@ -131,6 +131,7 @@ struct MoveWorkspace {
     // global-table path (13..18), and the cluster-table fill (MG_FILL_*)
     int giant_class = kFirstHeavyClass + kTiers - 1;
     int cluster_fill = MG_FILL_AUTO;
+    int coarsen_combine = MG_COMBINE_AUTO;  // MG_COMBINE_*, read by the coarsening of a run
     // heavy-vertex global tables
     DBuf<uint64_t> h_toff;         // table offset per heavy vertex (H+1)
     DBuf<uint32_t> h_tsize;        // table size per heavy vertex
@@ -169,6 +170,12 @@ struct SweepParams {
 // the agg flag of a sweep: the automatic choice unless the workspace forces a fill
 inline int sweep_agg(const MoveWorkspace &ws, int automatic) {
     return ws.cluster_fill == MG_FILL_OWN ? 0 : ws.cluster_fill == MG_FILL_SPLIT ? 1 : automatic;
+}
+// combining in the coarsening of a run: automatic when the phase's last sweep
+// saw at most one distinct candidate community per 4 edges
+inline bool coarsen_combine(const MoveWorkspace &ws, unsigned long long distinct, uint64_t nnz) {
+    return ws.coarsen_combine == MG_COMBINE_ON ||
+           (ws.coarsen_combine == MG_COMBINE_AUTO && 4 * distinct <= nnz);
 }
 
 // Constants of the gain of one graph, from its mass (sum of all directed
@@ -226,8 +233,10 @@ void move_sweep_batch(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &w
 // Shapes of the level's light classes from the tuning table; with MG_TUNE_ON,
 // classes missing from it are timed now with the sweep's arguments (P, N, k,
 // sigma as the next sweep will use them: the timing runs write the same N).
+// With timing = false the table is only read (classes missing from it keep
+// the built-in shapes).
 void move_tune(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p, const uint32_t *P,
-               uint32_t *N, const double *k, const double *sigma, cudaStream_t s);
+               uint32_t *N, const double *k, const double *sigma, cudaStream_t s, bool timing = true);
 void move_tune_batch(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p,
                      const BatchSweep &b, const double *k, const double *sigma, cudaStream_t s);
 void sweep_reset_acc(MoveWorkspace &ws, cudaStream_t s);
@@ -249,6 +258,7 @@ struct CoarsenWorkspace {
     DBuf<uint32_t> seg, rowcnt;
     DBuf<uint64_t> u64tmp;
     DBuf<uint32_t> u32tmp;
+    DBuf<uint32_t> tcount;  // combined entries per expansion tile
     PrimWorkspace prim;
 };
 // A device CSR level: f64 weights (w, wk = WK_F64), or exact 32-bit integer
@@ -276,8 +286,11 @@ void level_weights_f64(const GraphView &g, double *out, cudaStream_t s);
 // Dense order-preserving relabel; returns n'.
 uint32_t relabel_dense(const uint32_t *C, uint32_t n, uint32_t *C_dense, CoarsenWorkspace &ws, cudaStream_t s);
 // Next level from a graph and a dense assignment with n' communities.
+// combine: merge equal keys within each warp's 32 edges before sorting (pays
+// when communities repeat inside rows); the result does not depend on it.
 void coarsen_level(const GraphView &g, const uint32_t *C_dense, uint32_t n_new, int integral, LevelGraph &out,
-                   CoarsenWorkspace &ws, cudaStream_t s, uint64_t *upper_degree_off /* device, may be null */);
+                   CoarsenWorkspace &ws, cudaStream_t s, uint64_t *upper_degree_off /* device, may be null */,
+                   bool combine = false);
 
 // Build a symmetric deduplicated CSR from undirected pairs already on the
 // device (self-loops dropped); used by the generators.  With pair weights w

@@ -489,30 +489,37 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
                 if (wbase + b * GT >= hi) break;
                 const uint32_t c = cc[b];
                 uint32_t hnew = kEmpty;  // slot this lane claimed for a new key
-                if (jj[b] != kEmpty) {
-                    if (c != src) {
-                        if (is_candidate<VER>(c, src, up)) {
-                            uint32_t h = hash_slot(c, tb);
-                            for (uint32_t p = 0; p < S; p++) {
-                                const uint32_t cur = ((volatile uint32_t *)keys)[h];
-                                if (cur == c) break;
-                                if (cur == kEmpty) {
-                                    const uint32_t prev = atomicCAS(keys + h, kEmpty, c);
-                                    if (prev == kEmpty) {
-                                        hnew = h;
-                                        break;
-                                    }
-                                    if (prev == c) break;
-                                }
-                                h = (h + 1) & mask;
-                            }
-                            atomicAdd(vals + h, ww[b]);
-                        }
-                    } else if (jj[b] != i) {
-                        e_part += ww[b];
-                    } else {
-                        s_part += ww[b];
+                bool cand = jj[b] != kEmpty && c != src && is_candidate<VER>(c, src, up);
+                V wv = ww[b];
+                if constexpr (kIntg<WK>) {
+                    // communities that repeat in the warp's edges (later sweeps):
+                    // equal keys add their weights in registers and one leader
+                    // inserts the sum (exact integer sums; uniform: a kernel argument)
+                    if (A.agg) {
+                        const uint32_t peers = __match_any_sync(0xffffffffu, cand ? c : kEmpty);
+                        wv = __reduce_add_sync(peers, wv);
+                        cand = cand && (uint32_t)(__ffs(peers) - 1) == lane;
                     }
+                }
+                if (cand) {
+                    uint32_t h = hash_slot(c, tb);
+                    for (uint32_t p = 0; p < S; p++) {
+                        const uint32_t cur = ((volatile uint32_t *)keys)[h];
+                        if (cur == c) break;
+                        if (cur == kEmpty) {
+                            const uint32_t prev = atomicCAS(keys + h, kEmpty, c);
+                            if (prev == kEmpty) {
+                                hnew = h;
+                                break;
+                            }
+                            if (prev == c) break;
+                        }
+                        h = (h + 1) & mask;
+                    }
+                    atomicAdd(vals + h, wv);
+                } else if (jj[b] != kEmpty && c == src) {
+                    if (jj[b] != i) e_part += ww[b];
+                    else s_part += ww[b];
                 }
                 // the warp's new slots join the table's list with one atomic
                 const uint32_t m = __ballot_sync(0xffffffffu, hnew != kEmpty);
@@ -1556,7 +1563,7 @@ inline std::vector<int> tune_candidates(int cls) {
 // the same new assignment the sweep will write; its sums go to ws.tune_acc.
 template <int BT>
 void tune_light(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p, LMArgs A,
-                cudaStream_t s) {
+                cudaStream_t s, bool timing = true) {
     for (int c = 0; c < kLightClasses; c++) lvl.shape[c] = (uint8_t)default_shape(c);
     TuneTable &T = ws.tune;
     if (T.mode == MG_TUNE_OFF) return;
@@ -1572,7 +1579,7 @@ void tune_light(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, const Swe
             lvl.shape[c] = it->second.shape;
             continue;
         }
-        if (T.mode != MG_TUNE_ON) continue;
+        if (T.mode != MG_TUNE_ON || !timing) continue;
         float best = 1e30f;
         int best_sh = default_shape(c);
         for (int sh : tune_candidates(c)) {

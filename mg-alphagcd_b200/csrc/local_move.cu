@@ -274,8 +274,8 @@ void move_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, con
 }
 
 void move_tune(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, const SweepParams &p, const uint32_t *P,
-               uint32_t *N, const double *k, const double *sigma, cudaStream_t s) {
-    tune_light<0>(g, lvl, ws, p, single_args(g, ws, p, P, N, k, sigma), s);
+               uint32_t *N, const double *k, const double *sigma, cudaStream_t s, bool timing) {
+    tune_light<0>(g, lvl, ws, p, single_args(g, ws, p, P, N, k, sigma), s, timing);
 }
 
 void sigma_sumsq(const double *sigma, uint32_t n, int integral, MoveWorkspace &ws, cudaStream_t s) {

@@ -139,9 +139,10 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
         // first sweep: P = identity (base), proposes C[1]; yields Q0
         sp.up = 1;
         sp.agg = sweep_agg(ctx->mws, 0);
-        // shapes of the light classes (autotuner; its timing runs write the
-        // proposal this sweep writes)
-        move_tune(cur, mlv, ctx->mws, sp, C[base], C[pend], k, sigma, s);
+        // shapes of the light classes from the tuning table; classes missing
+        // from it are timed on the level's second sweep, which is more like
+        // the rest of the level than the first (every community one vertex)
+        move_tune(cur, mlv, ctx->mws, sp, C[base], C[pend], k, sigma, s, false);
         sweep_reset_acc(ctx->mws, s);
         sigma_sumsq(sigma, n, integral, ctx->mws, s);
         MG_CUDA(cudaEventRecord(ctx->ev[4], s));
@@ -168,6 +169,8 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
             // than half of the last sweep's edges were distinct candidates
             sp.agg = sweep_agg(ctx->mws, 2 * hacc.distinct < cur.nnz);
             const int next = 3 - base - pend;
+            // autotuner: its timing runs write the proposal this sweep writes
+            if (loop == 0) move_tune(cur, mlv, ctx->mws, sp, C[pend], C[next], k, sigma, s, true);
             Timer ti(ctx->ev[0], ctx->ev[1], s);
             sweep_reset_acc(ctx->mws, s);
             sigma_sumsq(sigma, n, integral, ctx->mws, s);
@@ -220,7 +223,8 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
             S.seconds_coarsen += tc.stop_sync();
             break;
         }
-        coarsen_level(cur, Cd, nn, integral, ctx->lv[lvl_out], ctx->cws, s, nullptr);
+        coarsen_level(cur, Cd, nn, integral, ctx->lv[lvl_out], ctx->cws, s, nullptr,
+                      coarsen_combine(ctx->mws, hacc.distinct, cur.nnz));
         double ct = tc.stop_sync();
         S.seconds_coarsen += ct;
         if (verbose) printf("Coarsen graph execution time: %f s, %f ms\n", ct, ct * 1e3);

@@ -345,3 +345,51 @@ def test_level_graphs_equal_oracle_coarsening(O, ctx):
         assert (off == h.offsets).all() and (cols == h.cols).all() and (w == h.weights).all(), lvl
         cur = h
     assert "level_csr" not in dg.louvain(keep_levels=1)
+
+
+@pytest.mark.parametrize("combine", [1, 2])  # COMBINE_OFF, COMBINE_ON
+def test_coarsen_combine_modes_bit_exact(O, mg, ctx, combine):
+    """Coarsening with and without warp combining of equal keys gives the
+    oracle's next-level graph (integral weights exactly, real weights to
+    1e-12 relative), also for a phase's final assignment, where communities
+    repeat inside rows and combining merges most entries."""
+    ctx.sweep_options(coarsen_combine=combine)
+    try:
+        rng = np.random.default_rng(3)
+        base = O.gen_rmat(13, seed=3)
+        row = np.repeat(np.arange(base.n), np.diff(base.offsets).astype(np.int64))
+        m = row < base.cols
+        wint = O.csr_from_pairs(base.n, row[m], base.cols[m], rng.integers(1, 9, m.sum()).astype(np.float64))
+        for name, g in _graphs(O) + [("rmat13w", wint)]:
+            dg = _up(ctx, g)
+            k = O.vertex_weights(g)
+            states = [C for C, _ in _states(O, g, k, O.mass(g))]
+            states.append(O.louvain(g, max_phases=1)["assignment"].astype(np.uint32))
+            for C in states:
+                cd_a, g2 = dg.coarsen(C)
+                cd_b, h2, _ = O.coarsen(g, C)
+                assert (cd_a == cd_b).all(), name
+                off, cols, w = g2.csr()
+                assert (off == h2.offsets).all() and (cols == h2.cols).all(), name
+                assert (w == h2.weight_array()).all(), name
+        g = O.gen_chunglu(1 << 13, max_degree=1000.0, seed=4)
+        dg = _up(ctx, g)
+        for C in (np.random.default_rng(2).integers(0, 500, g.n).astype(np.uint32),
+                  O.louvain(g, max_phases=1)["assignment"].astype(np.uint32)):
+            _, g2 = dg.coarsen(C)
+            _, h2, _ = O.coarsen(g, C)
+            off, cols, w = g2.csr()
+            assert (off == h2.offsets).all() and (cols == h2.cols).all()
+            np.testing.assert_allclose(w, h2.weights, rtol=1e-12)
+    finally:
+        ctx.sweep_options()
+
+
+@pytest.mark.parametrize("combine", [1, 2])
+def test_louvain_combine_modes(O, ctx, combine):
+    ctx.sweep_options(coarsen_combine=combine)
+    try:
+        for name, g in [("sbm64k", O.gen_sbm(65536, 64, 16.0, 0.8, seed=1)), ("rmat14", O.gen_rmat(14, seed=2))]:
+            _compare_runs(_up(ctx, g).louvain(), O.louvain(g))
+    finally:
+        ctx.sweep_options()
