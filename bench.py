@@ -32,9 +32,11 @@ R-MAT-24 probabilities; vertex counts log-uniform in [1k, 8M]) submitted to
 the continuous-batching server (8 slots sharing a 150 GB HBM budget):
 offered and served jobs/s and the submit-to-done latency percentiles of the
 jobs completed within the window (jobs still queued at its end are reported
-with their count and age).  Its "sustained_load" entry repeats the window at
-a load one GPU keeps up with (default 6 requests/s for 30 s), where the
-latency percentiles measure service, not backlog.
+with their count and age).  Its "rate_ladder" repeats the window at lower
+loads (default 6, 10 and 14 requests/s for 15 s each), where the latency
+percentiles measure service rather than backlog; "sustained_load" is the
+first of them and "max_rate_p99_below_1s" the highest rate of the ladder
+that was served completely with p99 below one second.
 
 --impl reference times the reference's Louvain logic on the host cores (the
 CPU oracle port under OpenMP, all host threads): each step is one phase-0
@@ -85,9 +87,10 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--serve-slots", type=int, default=SERVE["slots"], help="worker slots of the server")
-    ap.add_argument("--sustain-rate", type=float, default=6.0,
-                    help="second serving window at a load the server can keep up with (0: skip)")
-    ap.add_argument("--sustain-seconds", type=float, default=30.0)
+    ap.add_argument("--sustain-rates", default="6,10,14",
+                    help="serving windows at lower loads (comma-separated req/s; empty: skip): the first is "
+                         "'sustained_load', all form 'rate_ladder' with the highest rate whose p99 stays below 1 s")
+    ap.add_argument("--sustain-seconds", type=float, default=15.0)
     return ap.parse_args()
 
 
@@ -629,11 +632,18 @@ def run_engine(args, world, rank, local, pg):
         g.close()
         ctx.close()  # the server's slots take the HBM budget
         serving = run_serving(mg, args.serve_rate, args.serve_seconds, local, args.serve_slots)
-        if args.sustain_rate > 0:
-            # the same job mix at a load one GPU keeps up with: latency is
+        rates = [float(x) for x in args.sustain_rates.split(",") if x.strip()]
+        if rates:
+            # the same job mix at loads one GPU keeps up with: latency is
             # service time plus short queueing, not backlog
-            serving["sustained_load"] = run_serving(mg, args.sustain_rate, args.sustain_seconds, local,
-                                                    args.serve_slots)
+            ladder = [run_serving(mg, r, args.sustain_seconds, local, args.serve_slots) for r in rates]
+            serving["sustained_load"] = ladder[0]
+            serving["rate_ladder"] = [{"offered_jobs_per_s": x["offered_jobs_per_s"],
+                                       "served_jobs_per_s": x["served_jobs_per_s"],
+                                       "p50_latency_s": x["p50_latency_s"], "p99_latency_s": x["p99_latency_s"],
+                                       "unfinished": x["unfinished"]} for x in ladder]
+            ok = [x["offered_jobs_per_s"] for x in ladder if x["p99_latency_s"] < 1.0 and x["unfinished"] == 0]
+            serving["max_rate_p99_below_1s"] = max(ok) if ok else None
     if rank != 0:
         return None
     line = {

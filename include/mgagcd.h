@@ -283,7 +283,7 @@ mg_status mg_tune_load(mg_ctx *ctx, const char *path);
  * the same result (bit for bit on integral weights); they exist for tuning and
  * so that tests can force each path. */
 enum {
-    MG_FILL_AUTO = 0,  /* own fill on a phase's first sweep, split fill once communities repeat */
+    MG_FILL_AUTO = 0,  /* the engine's choice: the own fill (measured faster on R-MAT-24 at every level) */
     MG_FILL_OWN = 1,   /* every CTA of a cluster reads the whole row and inserts the communities it owns */
     MG_FILL_SPLIT = 2  /* the CTAs split the row; equal communities combined in the warp; inserts via DSMEM */
 };
@@ -301,6 +301,7 @@ typedef struct {
     int cluster_fill;    /* MG_FILL_* */
     int giant_class;     /* degree classes >= this (13..18) take the global-table path; 0 = default (18) */
     int coarsen_combine; /* MG_COMBINE_* */
+    int light_streams;   /* streams the light degree classes are spread over, 1..7 (0 = default 2) */
 } mg_sweep_opts;
 /* Set the context's policy (opts NULL = defaults); applies to later sweeps and runs. */
 mg_status mg_sweep_options(mg_ctx *ctx, const mg_sweep_opts *opts);

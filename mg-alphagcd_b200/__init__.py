@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import ctypes as ct
 import os
+import weakref
 from typing import Optional
 
 import numpy as np
@@ -49,7 +50,8 @@ class _Opts(ct.Structure):
 
 
 class _SweepOpts(ct.Structure):
-    _fields_ = [("cluster_fill", ct.c_int), ("giant_class", ct.c_int), ("coarsen_combine", ct.c_int)]
+    _fields_ = [("cluster_fill", ct.c_int), ("giant_class", ct.c_int), ("coarsen_combine", ct.c_int),
+                ("light_streams", ct.c_int)]
 
 
 class _RunOpts(ct.Structure):
@@ -227,9 +229,19 @@ class Context:
             raise MGError(st, f"{what}: {lib().mg_last_error(self.h).decode()}")
 
     def close(self):
+        """Destroy the context -- after the graphs and batches made on it,
+        which the C ABI requires to go first (they use its streams)."""
         if self.h:
+            for child in list(getattr(self, "_children", ())):
+                child.close()
             lib().mg_destroy(self.h)
             self.h = ct.c_void_p()
+
+    def _adopt(self, child):
+        if not hasattr(self, "_children"):
+            self._children = weakref.WeakSet()
+        self._children.add(child)
+        return child
 
     def __enter__(self):
         return self
@@ -308,12 +320,14 @@ class Context:
         self.check(lib().mg_tune_mode(self.h, mode), "mg_tune_mode")
 
     def sweep_options(self, cluster_fill: int = FILL_AUTO, giant_class: int = 0,
-                      coarsen_combine: int = COMBINE_AUTO):
+                      coarsen_combine: int = COMBINE_AUTO, light_streams: int = 0):
         """Sweep and coarsening policy (mg_sweep_options): the cluster-table
         fill (FILL_*), the first degree class (13..18, 0 = default) sent to
         the global-table path, and warp combining of equal keys in the
-        coarsening (COMBINE_*).  Results do not depend on it."""
-        o = _SweepOpts(cluster_fill, giant_class, coarsen_combine)
+        coarsening (COMBINE_*), and the number of streams the light degree
+        classes are spread over (1..7, 0 = default 2).  Results do not depend
+        on it."""
+        o = _SweepOpts(cluster_fill, giant_class, coarsen_combine, light_streams)
         self.check(lib().mg_sweep_options(self.h, ct.byref(o)), "mg_sweep_options")
 
     def tune_table(self) -> list:
@@ -541,6 +555,7 @@ class Batch:
     def __init__(self, ctx: Context, h: ct.c_void_p):
         self.ctx = ctx
         self.h = h
+        ctx._adopt(self)
 
     def close(self):
         if self.h:
@@ -599,6 +614,7 @@ class Graph:
     def __init__(self, ctx: Context, h: ct.c_void_p):
         self.ctx = ctx
         self.h = h
+        ctx._adopt(self)
 
     def close(self):
         if self.h:

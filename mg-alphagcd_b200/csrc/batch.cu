@@ -637,7 +637,8 @@ void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &re
             pg.reset();
         };
         bool plain = true;
-        B.sp.agg = sweep_agg(ctx->mws, 0);  // the phase's first sweep: every community is one vertex
+        B.sp.agg = 0;  // the phase's first sweep: every community is one vertex
+        B.sp.split = sweep_split(ctx->mws);
         while (true) {
             if (use_graph && !plain) {
                 if (!pg) {
@@ -653,7 +654,7 @@ void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &re
                 run_body(ctx, b, B, s, 0, cudaGraphConditionalHandle());
             }
             plain = false;
-            B.sp.agg = sweep_agg(ctx->mws, 1);  // later sweeps: communities repeat among neighbours
+            B.sp.agg = 1;  // later sweeps: communities repeat among neighbours
             MG_CUDA(cudaMemcpyAsync(W.h_ctrl, ctrl, sizeof(BatchCtrl), cudaMemcpyDeviceToHost, s));
             MG_CUDA(cudaStreamSynchronize(s));
             if (W.h_ctrl->active == 0) break;

@@ -406,7 +406,8 @@ mg_status mg_local_move(mg_graph *g, int version, int up, int precision, const u
         sp.precision = precision;
         sp.mass = g->mass;
         sp.integral = g->integral;
-        sp.agg = sweep_agg(ctx->mws, 0);
+        sp.agg = 0;
+        sp.split = sweep_split(ctx->mws);
         sweep_reset_acc(ctx->mws, s);
         move_sweep(g->view(), lvl, ctx->mws, sp, dC, dN, dk, ds, s);
         MG_CUDA(cudaMemcpyAsync(C_new, dN, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));
@@ -617,6 +618,8 @@ mg_status mg_sweep_options(mg_ctx *ctx, const mg_sweep_opts *opts) {
     const int comb = opts ? opts->coarsen_combine : MG_COMBINE_AUTO;
     if (comb < MG_COMBINE_AUTO || comb > MG_COMBINE_ON)
         return fail(ctx, MG_ERR_INVALID, "mg_sweep_options: unknown coarsen_combine");
+    if (opts && (opts->light_streams < 0 || opts->light_streams > MoveWorkspace::kStreams - 1))
+        return fail(ctx, MG_ERR_INVALID, "mg_sweep_options: light_streams must be 0..7");
     const int gc = opts && opts->giant_class ? opts->giant_class : kFirstHeavyClass + kTiers - 1;
     if (fill < MG_FILL_AUTO || fill > MG_FILL_SPLIT) return fail(ctx, MG_ERR_INVALID, "mg_sweep_options: unknown fill");
     if (gc < kFirstHeavyClass || gc > kFirstHeavyClass + kTiers - 1)
@@ -624,6 +627,8 @@ mg_status mg_sweep_options(mg_ctx *ctx, const mg_sweep_opts *opts) {
     ctx->mws.cluster_fill = fill;
     ctx->mws.giant_class = gc;
     ctx->mws.coarsen_combine = comb;
+    ctx->mws.light_streams =
+        opts && opts->light_streams ? opts->light_streams : MoveWorkspace::kDefaultLightStreams;
     return MG_OK;
 }
 

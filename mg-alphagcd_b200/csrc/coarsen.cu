@@ -497,10 +497,12 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
     uint32_t *ustart, *seg, *head;
     uint32_t u = unique_runs(sk, mm, bc, n_new, out, ws, s, &ustart, &seg, &head);
     if (integral && !weighted) {
-        run_lengths_kernel<uint32_t><<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)mm, out.wi.ensure(u + 1));
+        uint32_t *wi = out.wi.ensure(u + 1);  // (allocations stay out of launch argument lists)
+        run_lengths_kernel<uint32_t><<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)mm, wi);
         MG_LAUNCH_CHECK();
     } else if (!weighted) {
-        run_lengths_kernel<double><<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)mm, out.w.ensure(u + 1));
+        double *w = out.w.ensure(u + 1);
+        run_lengths_kernel<double><<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)mm, w);
         MG_LAUNCH_CHECK();
     } else if (integral) {
         // exact: 64-bit prefix sums over the sorted weights, run sum = difference
@@ -508,7 +510,8 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
         to_u64_kernel<uint32_t><<<grid_for(mm), 256, 0, s>>>(flipped ? ivals2 : ivals, mm, pre);
         MG_LAUNCH_CHECK();
         exclusive_scan<uint64_t>(pre, pre, mm, pre + mm, s, ws.prim);
-        run_diff_kernel<<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)mm, pre, out.wi.ensure(u + 1));
+        uint32_t *wi = out.wi.ensure(u + 1);
+        run_diff_kernel<<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)mm, pre, wi);
         MG_LAUNCH_CHECK();
     } else {
         double *w = out.w.ensure(u + 1);
@@ -573,7 +576,8 @@ void csr_from_device_pairs(uint32_t n, uint64_t m, const uint32_t *u, const uint
     } else {
         emit_rows(ukey, uu, bc, n, off, col, s);
         if (w) {
-            run_first_values_kernel<<<grid_for(uu), 256, 0, s>>>(ustart, uu, sv, out.w.ensure((size_t)uu + 1));
+            double *w = out.w.ensure((size_t)uu + 1);
+            run_first_values_kernel<<<grid_for(uu), 256, 0, s>>>(ustart, uu, sv, w);
             MG_LAUNCH_CHECK();
         }
     }

@@ -146,8 +146,14 @@ struct MoveWorkspace {
     DBuf<SweepAcc> tune_acc;       // sums of the autotuner's timing runs (discarded)
     TuneTable tune;
     PrimWorkspace prim;
-    cudaStream_t streams[4] = {nullptr, nullptr, nullptr, nullptr};
-    cudaEvent_t ev_fork = nullptr, ev_join[4] = {nullptr, nullptr, nullptr, nullptr};
+    // stream 0: heavy tiers; streams 1..light_streams: the light classes and
+    // the 1-CTA cluster tier, so that one class's tail overlaps the others
+    // (two by default: more streams measured slower on R-MAT-24)
+    static constexpr int kStreams = 8;
+    static constexpr int kDefaultLightStreams = 2;
+    cudaStream_t streams[kStreams] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join[kStreams] = {};
+    int light_streams = kDefaultLightStreams;
     cudaEvent_t ev_tune[2] = {nullptr, nullptr};  // timing events of the autotuner
     ~MoveWorkspace();
     void init_streams();
@@ -166,11 +172,11 @@ struct SweepParams {
     // set from the previous sweep's distinct candidates per edge (never on the
     // first sweep of a phase, where every community is one vertex).
     int agg = 0;
+    // cluster tables: split fill with warp combining (MG_FILL_SPLIT) instead
+    // of the own fill
+    int split = 0;
 };
-// the agg flag of a sweep: the automatic choice unless the workspace forces a fill
-inline int sweep_agg(const MoveWorkspace &ws, int automatic) {
-    return ws.cluster_fill == MG_FILL_OWN ? 0 : ws.cluster_fill == MG_FILL_SPLIT ? 1 : automatic;
-}
+inline int sweep_split(const MoveWorkspace &ws) { return ws.cluster_fill == MG_FILL_SPLIT; }
 // combining in the coarsening of a run: automatic when the phase's last sweep
 // saw at most one distinct candidate community per 4 edges
 inline bool coarsen_combine(const MoveWorkspace &ws, unsigned long long distinct, uint64_t nnz) {

@@ -477,7 +477,8 @@ void graph_generate_chunglu(mg_graph *g, uint32_t n, double exponent, double mea
     } else {
         // every weight is a float value: keep them as f32
         if (lv.nnz) {
-            to_f32_kernel<<<148 * 16, 256, 0, s>>>(lv.w.get(), lv.nnz, g->w32.ensure(lv.nnz + 1));
+            float *w32 = g->w32.ensure(lv.nnz + 1);  // (allocations stay out of launch argument lists)
+            to_f32_kernel<<<148 * 16, 256, 0, s>>>(lv.w.get(), lv.nnz, w32);
             MG_LAUNCH_CHECK();
         }
         g->wk = WK_F32;
@@ -656,7 +657,8 @@ void batch_from_host_csr(mg_batch *b, const uint64_t *voff, const uint64_t *offs
         MG_CUDA(cudaMemcpyAsync(dvoff, b->voff.data(), sizeof(uint32_t) * (G + 1), cudaMemcpyHostToDevice, s));
         uint32_t *dcol = u->col.ensure(nnz + 1);
         if (nnz) MG_CUDA(cudaMemcpyAsync(dcol, cols, sizeof(uint32_t) * nnz, cudaMemcpyHostToDevice, s));
-        batch_rows_kernel<<<148 * 16, 256, 0, s>>>(d64, (uint32_t)n, dvoff, G, dcol, u->off.ensure(n + 1), dbad);
+        uint32_t *uoff = u->off.ensure(n + 1);  // (allocations stay out of launch argument lists)
+        batch_rows_kernel<<<148 * 16, 256, 0, s>>>(d64, (uint32_t)n, dvoff, G, dcol, uoff, dbad);
         MG_LAUNCH_CHECK();
         int hbad = 0;
         MG_CUDA(cudaMemcpyAsync(&hbad, dbad, sizeof(int), cudaMemcpyDeviceToHost, s));

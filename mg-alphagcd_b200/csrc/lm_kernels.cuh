@@ -33,7 +33,8 @@ struct LMArgs {
     GainK K;             // gain constants of the graph
     int up;
     int integral;
-    int agg;             // combine equal communities in the warp before inserting (cluster tables)
+    int agg;             // communities repeat among neighbours: lane-local run combining (table kernels)
+    int split;           // cluster tables: split rows over the CTAs, combine in the warp, insert via DSMEM
     SweepAcc *acc;
     // batched sweeps: graph of each vertex, per-graph control word and gain
     // constants, the three assignment buffers, sum_in per vertex, and the
@@ -470,6 +471,42 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
         // warp-uniform loop bound (lanes past the row's end take part with no
         // edge), so that the warp can append its new slots with one atomic
         const uint32_t lane = threadIdx.x & 31u;
+        // add `val` to community `key`'s slot (kEmpty: nothing); called by
+        // every lane of the warp at the same point, so that the warp's new
+        // slots join the table's candidate list with one atomic
+        auto insert = [&](uint32_t key, V val) {
+            uint32_t hnew = kEmpty;  // slot this lane claimed for a new key
+            if (key != kEmpty) {
+                // one compare-and-swap per probe: claims an empty slot or
+                // finds the key (load <= 1/2, so the loop ends long before S)
+                uint32_t h = hash_slot(key, tb);
+                for (uint32_t p = 0; p < S; p++) {
+                    const uint32_t prev = atomicCAS(keys + h, kEmpty, key);
+                    if (prev == kEmpty) {
+                        hnew = h;
+                        break;
+                    }
+                    if (prev == key) break;
+                    h = (h + 1) & mask;
+                }
+                atomicAdd(vals + h, val);
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, hnew != kEmpty);
+            if (m) {
+                const uint32_t leader = __ffs(m) - 1;
+                uint32_t pos = 0;
+                if (lane == leader) pos = atomicAdd(&cnt[par][g], (uint32_t)__popc(m));
+                pos = __shfl_sync(0xffffffffu, pos, leader);
+                if (hnew != kEmpty) used[pos + __popc(m & ((1u << lane) - 1u))] = (uint16_t)hnew;
+            }
+        };
+        // run combining (A.agg: sweeps where communities repeat): a lane adds
+        // the weights of its consecutive edges into one community in a
+        // register and inserts the sum when its community changes, so rows
+        // whose neighbours sit in a few communities make few shared-memory
+        // adds to the same slot
+        uint32_t rk = kEmpty;
+        V rs = V(0);
         for (uint32_t wbase = lo + (t & ~31u); wbase < hi; wbase += GT * BATCH) {
             const uint32_t base = wbase + lane;
             uint32_t jj[BATCH], cc[BATCH];
@@ -488,50 +525,26 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
             for (int b = 0; b < BATCH; b++) {
                 if (wbase + b * GT >= hi) break;
                 const uint32_t c = cc[b];
-                uint32_t hnew = kEmpty;  // slot this lane claimed for a new key
-                bool cand = jj[b] != kEmpty && c != src && is_candidate<VER>(c, src, up);
-                V wv = ww[b];
-                if constexpr (kIntg<WK>) {
-                    // communities that repeat in the warp's edges (later sweeps):
-                    // equal keys add their weights in registers and one leader
-                    // inserts the sum (exact integer sums; uniform: a kernel argument)
-                    if (A.agg) {
-                        const uint32_t peers = __match_any_sync(0xffffffffu, cand ? c : kEmpty);
-                        wv = __reduce_add_sync(peers, wv);
-                        cand = cand && (uint32_t)(__ffs(peers) - 1) == lane;
+                const bool cand = jj[b] != kEmpty && c != src && is_candidate<VER>(c, src, up);
+                if (A.agg) {  // uniform: a kernel argument
+                    const bool same = cand && c == rk;
+                    const uint32_t fk = cand && !same ? rk : kEmpty;
+                    const V fv = rs;
+                    if (cand) {
+                        rs = same ? rs + ww[b] : ww[b];
+                        rk = c;
                     }
+                    insert(fk, fv);
+                } else {
+                    insert(cand ? c : kEmpty, ww[b]);
                 }
-                if (cand) {
-                    uint32_t h = hash_slot(c, tb);
-                    for (uint32_t p = 0; p < S; p++) {
-                        const uint32_t cur = ((volatile uint32_t *)keys)[h];
-                        if (cur == c) break;
-                        if (cur == kEmpty) {
-                            const uint32_t prev = atomicCAS(keys + h, kEmpty, c);
-                            if (prev == kEmpty) {
-                                hnew = h;
-                                break;
-                            }
-                            if (prev == c) break;
-                        }
-                        h = (h + 1) & mask;
-                    }
-                    atomicAdd(vals + h, wv);
-                } else if (jj[b] != kEmpty && c == src) {
+                if (!cand && jj[b] != kEmpty && c == src) {
                     if (jj[b] != i) e_part += ww[b];
                     else s_part += ww[b];
                 }
-                // the warp's new slots join the table's list with one atomic
-                const uint32_t m = __ballot_sync(0xffffffffu, hnew != kEmpty);
-                if (m) {
-                    const uint32_t leader = __ffs(m) - 1;
-                    uint32_t pos = 0;
-                    if (lane == leader) pos = atomicAdd(&cnt[par][g], (uint32_t)__popc(m));
-                    pos = __shfl_sync(0xffffffffu, pos, leader);
-                    if (hnew != kEmpty) used[pos + __popc(m & ((1u << lane) - 1u))] = (uint16_t)hnew;
-                }
             }
         }
+        if (A.agg) insert(rk, rs);  // every lane's last run
         // group totals of e and self weight, folded into the barrier that
         // publishes the table
         e_part = warp_sum(e_part);
@@ -938,16 +951,17 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
         const uint32_t lo = A.off[i], hi = A.off[i + 1], src = vv.P[i];
         const double ki = A.k[i];
         double e_part = 0, s_part = 0;
-        // Two ways to fill the cluster's table, chosen per sweep:
-        //  * distinct-heavy sweeps (no combining): every CTA reads the whole row
+        // Two ways to fill the cluster's table (mg_sweep_options; own by default,
+        // measured faster on R-MAT-24 at every level):
+        //  * own fill: every CTA reads the whole row
         //    (it stays in cache) and inserts only the communities whose slots
         //    it owns, so all table atomics are local;
-        //  * sweeps where communities repeat (A.agg): the CTAs split the row,
-        //    the warp combines equal communities, and the few remaining
-        //    inserts go to the owner CTA through distributed shared memory.
+        //  * split fill (A.split): the CTAs split the row, the warp combines
+        //    equal communities, and the few remaining inserts go to the owner
+        //    CTA through distributed shared memory.
         // The loop bound is warp-uniform (lanes past the row's end take part
         // with no edge), so that the warp can combine equal communities.
-        const bool own = CS > 1 && !A.agg;
+        const bool own = CS > 1 && !A.split;
         const uint32_t t0 = own ? threadIdx.x : rank * kClusterThreads + threadIdx.x;
         const uint32_t step = own ? kClusterThreads : CS * kClusterThreads;
         for (uint32_t wbase = lo + (t0 & ~31u); wbase < hi; wbase += step * BATCH) {
@@ -984,7 +998,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
                     // lanes holding the same community add their weights in the
                     // warp; one leader per community inserts the sum (integer
                     // sums: the result does not depend on the grouping)
-                    if (A.agg) {  // uniform: a kernel argument
+                    if (A.split) {  // uniform: a kernel argument
                         const uint32_t peers = __match_any_sync(0xffffffffu, cand ? c : kEmpty);
                         wv = __reduce_add_sync(peers, wv);
                         cand = cand && (uint32_t)(__ffs(peers) - 1) == (threadIdx.x & 31u);
@@ -1415,8 +1429,9 @@ void launch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, c
     const Bins &B = lvl.bins;
     // fork: heavy path on its own stream, the light classes on two others
     MG_CUDA(cudaEventRecord(ws.ev_fork, s));
-    for (int q = 0; q < 3; q++) MG_CUDA(cudaStreamWaitEvent(ws.streams[q], ws.ev_fork, 0));
-    cudaStream_t sh = ws.streams[0], sm = ws.streams[1], st = ws.streams[2];
+    const int ns = 1 + std::max(1, std::min(ws.light_streams, MoveWorkspace::kStreams - 1));
+    for (int q = 0; q < ns; q++) MG_CUDA(cudaStreamWaitEvent(ws.streams[q], ws.ev_fork, 0));
+    cudaStream_t sh = ws.streams[0], sm = ws.streams[1];
     const uint32_t *hl = lvl.heavy_list;
     // heavy tiers, largest clusters first
     if (lvl.tier_off[5] > lvl.tier_off[4])
@@ -1444,13 +1459,12 @@ void launch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, c
                                                                                   ws.h_acc.get(), ws.h_best.get());
         MG_LAUNCH_CHECK();
     }
-    // light classes, heaviest first; tiles and warp tables on one stream,
-    // block tables on the other
+    // light classes, heaviest first, spread over the light streams
     for (int c = kLightClasses - 1; c >= 0; c--) {
         const int sh_c = lvl.shape[c];
-        launch_light<WK, PREC, VER, BT>(sh_c, c, A, B.offset[c], B.size[c], sh_c <= SH_H32 ? st : sm);
+        launch_light<WK, PREC, VER, BT>(sh_c, c, A, B.offset[c], B.size[c], ws.streams[1 + c % (ns - 1)]);
     }
-    for (int q = 0; q < 3; q++) {
+    for (int q = 0; q < ns; q++) {
         MG_CUDA(cudaEventRecord(ws.ev_join[q], ws.streams[q]));
         MG_CUDA(cudaStreamWaitEvent(s, ws.ev_join[q], 0));
     }

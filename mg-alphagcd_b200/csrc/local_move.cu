@@ -259,6 +259,7 @@ LMArgs single_args(const GraphView &g, MoveWorkspace &ws, const SweepParams &p, 
     A.up = p.up;
     A.integral = p.integral;
     A.agg = p.agg;
+    A.split = p.split;
     A.acc = ws.acc.ensure(1);
     if (p.precision == MG_PREC_INT64)
         MG_CHECK(p.integral && p.mass < 2147483648.0, MG_ERR_UNSUPPORTED,
@@ -281,7 +282,8 @@ void move_tune(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, const Swee
 void sigma_sumsq(const double *sigma, uint32_t n, int integral, MoveWorkspace &ws, cudaStream_t s) {
     if (n == 0) return;
     unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(n, 256), 148ull * 8);
-    sigma_sumsq_kernel<<<grid, 256, 0, s>>>(sigma, n, integral, ws.acc.ensure(1));
+    SweepAcc *acc = ws.acc.ensure(1);  // (allocations stay out of launch argument lists)
+    sigma_sumsq_kernel<<<grid, 256, 0, s>>>(sigma, n, integral, acc);
     MG_LAUNCH_CHECK();
 }
 
@@ -289,7 +291,8 @@ void sigma_update(const uint32_t *P, const uint32_t *N, const double *k, double 
                   MoveWorkspace &ws, cudaStream_t s) {
     if (n == 0) return;
     unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(n, 256), 148ull * 8);
-    sigma_update_kernel<<<grid, 256, 0, s>>>(P, N, k, sigma, n, ws.acc.ensure(1));
+    SweepAcc *acc = ws.acc.ensure(1);
+    sigma_update_kernel<<<grid, 256, 0, s>>>(P, N, k, sigma, n, acc);
     MG_LAUNCH_CHECK();
 }
 

@@ -24,6 +24,7 @@ LMArgs batch_args(const GraphView &g, MoveWorkspace &ws, const SweepParams &p, c
     A.pgid = b.pgid;
     A.integral = p.integral;
     A.agg = p.agg;
+    A.split = p.split;
     A.acc = ws.acc.ensure(1);
     A.gid = b.gid;
     A.gword = b.gword;

@@ -4,12 +4,13 @@
 # oracle/ref_shim/ standing in for NVSHMEM and MPI.  Test infrastructure only:
 # the harness produces the golden vectors under tests/golden/.
 #
-# Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
+# Usage: oracle/build_ref.sh [reference_root]
+#   reference_root: the argument, else $MG_REFERENCE_ROOT, else /root/reference
 # Flags follow the reference's CMakeLists.txt (-O3, -Xcompiler -fopenmp,
 # separable compilation, -DTIMING, -D_FORCE_INLINES), with sm_100a as target.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${MG_REFERENCE_ROOT:-/root/reference}}"
 OUT="$HERE/_ref"
 if [ ! -d "$REF/src" ]; then
   echo "build_ref: no reference tree at $REF (skipped)" >&2

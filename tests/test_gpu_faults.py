@@ -86,7 +86,11 @@ def test_batch_survives_failed_allocations(O, mg):
     def attempt():
         c = mg.Context(0)
         try:
-            c.batch_from_csr([(g.n, g.offsets, g.cols, None) for g in gs]).run()
+            b = c.batch_from_csr([(g.n, g.offsets, g.cols, None) for g in gs])
+            try:
+                b.run()
+            finally:
+                b.close()
         finally:
             c.close()
 
