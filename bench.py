@@ -204,16 +204,21 @@ def peaks():
         return 6650.0, "fallback"
 
 
+TRAFFIC_PROFILE = "local_move_first_sweep_traffic"
+
+
 def traffic_per_sweep():
-    """DRAM bytes of the first level-0 sweep from the committed ncu summary,
-    with the algorithmic bytes of that same sweep (or Nones)."""
-    path = os.path.join(ROOT, "profiles", "local_move_rmat24_traffic.json")
+    """DRAM bytes of the first level-0 sweep of R-MAT-24 from the committed
+    ncu summary (measured on a smaller R-MAT and scaled by the entry count),
+    the algorithmic bytes of that sweep, and where the figure comes from."""
     try:
-        with open(path) as f:
+        with open(os.path.join(ROOT, "profiles", TRAFFIC_PROFILE + ".json")) as f:
             p = json.load(f)
-        return p.get("dram_bytes_per_sweep"), p.get("algorithmic_bytes_per_sweep")
-    except (OSError, ValueError):
-        return None, None
+        src = {"profile": p["key"], "measured_at_commit": p["measured_at_commit"], "scaling": p["scaling"],
+               "captures": {k: {"dram_bytes": v["dram_bytes"], "ratio": v["ratio"]} for k, v in p["captures"].items()}}
+        return p["rmat24_dram_bytes_scaled"], p["rmat24_algorithmic_bytes"], src
+    except (OSError, ValueError, KeyError):
+        return None, None, None
 
 
 def pinned_csr(g):
@@ -588,7 +593,7 @@ def run_engine(args, world, rank, local, pg):
     sweeps = sum(r["sweeps"] for r in runs)
     achieved = sweep_b / sweep_s / 1e9
     peak, peak_kind = peaks()
-    traffic, traffic_alg = traffic_per_sweep()
+    traffic, traffic_alg, traffic_src = traffic_per_sweep()
 
     # end to end through the public API with host buffers: upload the CSR
     # from pinned host memory, run, read the assignment back
@@ -660,8 +665,8 @@ def run_engine(args, world, rank, local, pg):
         "local_move_s": last["seconds_local_move"], "coarsen_s": last["seconds_coarsen"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "traffic_sweep": "first level-0 sweep (ncu, profiles/local_move_rmat24_traffic.md)",
-                     "traffic_sweep_algorithmic_bytes": traffic_alg,
+                     "traffic_sweep": "first level-0 sweep", "traffic_sweep_algorithmic_bytes": traffic_alg,
+                     "traffic_source": traffic_src,
                      "kernel": "local-move sweep (all bins)", "peak_kind": peak_kind,
                      "sweeps": sweeps, "algorithmic_bytes_per_sweep": sweep_b / max(sweeps, 1)},
         "cpu_baseline": cpu,

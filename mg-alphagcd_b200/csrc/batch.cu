@@ -638,7 +638,7 @@ void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &re
         };
         bool plain = true;
         B.sp.agg = 0;  // the phase's first sweep: every community is one vertex
-        B.sp.split = sweep_split(ctx->mws);
+        B.sp.split = sweep_split(ctx->mws, 0);
         while (true) {
             if (use_graph && !plain) {
                 if (!pg) {
@@ -655,6 +655,7 @@ void batch_run(mg_batch *b, const mg_run_opts &o, int flags, mg_batch_result &re
             }
             plain = false;
             B.sp.agg = 1;  // later sweeps: communities repeat among neighbours
+            B.sp.split = sweep_split(ctx->mws, 1);
             MG_CUDA(cudaMemcpyAsync(W.h_ctrl, ctrl, sizeof(BatchCtrl), cudaMemcpyDeviceToHost, s));
             MG_CUDA(cudaStreamSynchronize(s));
             if (W.h_ctrl->active == 0) break;

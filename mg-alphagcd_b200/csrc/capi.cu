@@ -407,7 +407,7 @@ mg_status mg_local_move(mg_graph *g, int version, int up, int precision, const u
         sp.mass = g->mass;
         sp.integral = g->integral;
         sp.agg = 0;
-        sp.split = sweep_split(ctx->mws);
+        sp.split = sweep_split(ctx->mws, 0);
         sweep_reset_acc(ctx->mws, s);
         move_sweep(g->view(), lvl, ctx->mws, sp, dC, dN, dk, ds, s);
         MG_CUDA(cudaMemcpyAsync(C_new, dN, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, s));

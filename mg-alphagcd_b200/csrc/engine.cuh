@@ -165,18 +165,19 @@ struct SweepParams {
     int precision = MG_PREC_FP64;
     double mass = 0;
     int integral = 0;
-    // combine neighbours of equal community inside a warp before inserting
-    // into the cluster tables (integral weights), where many threads of a
-    // heavy vertex otherwise add to the same slot.  Pays when many neighbours
-    // share communities;
-    // set from the previous sweep's distinct candidates per edge (never on the
-    // first sweep of a phase, where every community is one vertex).
+    // communities repeat among neighbours: the table kernels add a thread's
+    // consecutive edges into one community in a register before inserting
+    // (fewer shared-memory adds to one slot); set from the previous sweep's
+    // distinct candidates per edge (never on the first sweep of a phase,
+    // where every community is one vertex)
     int agg = 0;
     // cluster tables: split fill with warp combining (MG_FILL_SPLIT) instead
     // of the own fill
     int split = 0;
 };
-inline int sweep_split(const MoveWorkspace &ws) { return ws.cluster_fill == MG_FILL_SPLIT; }
+// split fill only when forced: the own fill measured faster on R-MAT-24 at
+// every level (also against splitting the sweeps where communities repeat)
+inline int sweep_split(const MoveWorkspace &ws, int /*agg*/) { return ws.cluster_fill == MG_FILL_SPLIT; }
 // combining in the coarsening of a run: automatic when the phase's last sweep
 // saw at most one distinct candidate community per 4 edges
 inline bool coarsen_combine(const MoveWorkspace &ws, unsigned long long distinct, uint64_t nnz) {

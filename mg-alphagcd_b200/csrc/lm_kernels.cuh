@@ -956,14 +956,44 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
         //  * own fill: every CTA reads the whole row
         //    (it stays in cache) and inserts only the communities whose slots
         //    it owns, so all table atomics are local;
-        //  * split fill (A.split): the CTAs split the row, the warp combines
-        //    equal communities, and the few remaining inserts go to the owner
-        //    CTA through distributed shared memory.
-        // The loop bound is warp-uniform (lanes past the row's end take part
-        // with no edge), so that the warp can combine equal communities.
+        //  * split fill (A.split): the CTAs split the row and the inserts go to
+        //    the owner CTA, through distributed shared memory when it is
+        //    another.
         const bool own = CS > 1 && !A.split;
         const uint32_t t0 = own ? threadIdx.x : rank * kClusterThreads + threadIdx.x;
         const uint32_t step = own ? kClusterThreads : CS * kClusterThreads;
+        // add `val` to community `key`'s slot in the segment of its owner CTA
+        // (this CTA's own shared memory, or another's through DSMEM)
+        auto ins = [&](uint32_t key, CV val) {
+            const uint32_t h = hash_range(key, (uint32_t)CS * S);
+            const unsigned owner = h / S;
+            uint32_t s = h & (S - 1);
+            uint32_t *ks = owner == rank ? keys : rank_ptr<CS>(keys, owner);
+            CV *vs = owner == rank ? vals : rank_ptr<CS>(vals, owner);
+            uint16_t *useg = owner == rank ? used : rank_ptr<CS>(used, owner);
+            uint32_t *uc = owner == rank ? &ucnt : rank_ptr<CS>(&ucnt, owner);
+            bool placed = false;
+            for (int p = 0; p < S; p++) {
+                const uint32_t prev = atomicCAS(ks + s, kEmpty, key);
+                if (prev == kEmpty) {
+                    useg[atomicAdd(uc, 1u)] = (uint16_t)s;
+                    placed = true;
+                    break;
+                }
+                if (prev == key) {
+                    placed = true;
+                    break;
+                }
+                s = (s + 1) & (S - 1);
+            }
+            if (placed) atomicAdd(vs + s, val);
+            else atomicAdd(&A.acc->overflow, 1ull);
+        };
+        // run combining (A.agg: sweeps where communities repeat): a thread adds
+        // the weights of its consecutive edges into one community and inserts
+        // the sum when its community changes
+        uint32_t rk = kEmpty;
+        CV rs = CV(0);
         for (uint32_t wbase = lo + (t0 & ~31u); wbase < hi; wbase += step * BATCH) {
             const uint32_t base = wbase + (t0 & 31u);
             uint32_t jj[BATCH], cc[BATCH];
@@ -980,60 +1010,28 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
             for (int b = 0; b < BATCH; b++) {
                 if (wbase + b * step >= hi) break;  // uniform over the warp
                 const uint32_t c = cc[b];
-                uint32_t s = 0;
-                unsigned owner = 0;
                 bool cand = jj[b] != kEmpty && c != src && is_candidate<VER>(c, src, up);
-                if (cand) {
-                    const uint32_t h = hash_range(c, (uint32_t)CS * S);
-                    owner = h / S;
-                    s = h & (S - 1);
-                    if (own) cand = owner == rank;
-                }
+                if (cand && own) cand = hash_range(c, (uint32_t)CS * S) / S == rank;
                 if ((!own || rank == 0) && jj[b] != kEmpty && c == src) {
                     if (jj[b] != i) e_part += ww[b];
                     else s_part += ww[b];
                 }
-                CV wv = cand ? wcast<CV>(ww[b]) : CV(0);
-                if constexpr (kIntg<WK>) {
-                    // lanes holding the same community add their weights in the
-                    // warp; one leader per community inserts the sum (integer
-                    // sums: the result does not depend on the grouping)
-                    if (A.split) {  // uniform: a kernel argument
-                        const uint32_t peers = __match_any_sync(0xffffffffu, cand ? c : kEmpty);
-                        wv = __reduce_add_sync(peers, wv);
-                        cand = cand && (uint32_t)(__ffs(peers) - 1) == (threadIdx.x & 31u);
-                    }
-                }
                 if (!cand) continue;
-                uint32_t *ks = own ? keys : rank_ptr<CS>(keys, owner);
-                CV *vs = own ? vals : rank_ptr<CS>(vals, owner);
-                uint16_t *useg = own ? used : rank_ptr<CS>(used, owner);
-                uint32_t *uc = own ? &ucnt : rank_ptr<CS>(&ucnt, owner);
-                bool placed = false;
-                for (int p = 0; p < S; p++) {
-                    uint32_t cur = ((volatile uint32_t *)ks)[s];
-                    if (cur == c) {
-                        placed = true;
-                        break;
+                const CV wv = wcast<CV>(ww[b]);
+                if (A.agg) {  // uniform: a kernel argument
+                    if (c == rk) {
+                        rs += wv;
+                    } else {
+                        if (rk != kEmpty) ins(rk, rs);
+                        rk = c;
+                        rs = wv;
                     }
-                    if (cur == kEmpty) {
-                        uint32_t prev = atomicCAS(ks + s, kEmpty, c);
-                        if (prev == kEmpty) {
-                            useg[atomicAdd(uc, 1u)] = (uint16_t)s;
-                            placed = true;
-                            break;
-                        }
-                        if (prev == c) {
-                            placed = true;
-                            break;
-                        }
-                    }
-                    s = (s + 1) & (S - 1);
+                } else {
+                    ins(c, wv);
                 }
-                if (placed) atomicAdd(vs + s, wv);
-                else atomicAdd(&A.acc->overflow, 1ull);
             }
         }
+        if (rk != kEmpty) ins(rk, rs);  // the thread's last run
         e_part = warp_sum(e_part);
         s_part = warp_sum(s_part);
         if ((threadIdx.x & 31) == 0) {

@@ -139,7 +139,7 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
         // first sweep: P = identity (base), proposes C[1]; yields Q0
         sp.up = 1;
         sp.agg = 0;
-        sp.split = sweep_split(ctx->mws);
+        sp.split = sweep_split(ctx->mws, 0);
         // shapes of the light classes from the tuning table; classes missing
         // from it are timed on the level's second sweep, which is more like
         // the rest of the level than the first (every community one vertex)
@@ -169,6 +169,7 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
             // combine equal communities in the warp once they repeat: fewer
             // than half of the last sweep's edges were distinct candidates
             sp.agg = 2 * hacc.distinct < cur.nnz;
+            sp.split = sweep_split(ctx->mws, sp.agg);
             const int next = 3 - base - pend;
             // autotuner: its timing runs write the proposal this sweep writes
             if (loop == 0) move_tune(cur, mlv, ctx->mws, sp, C[pend], C[next], k, sigma, s, true);
