@@ -51,7 +51,7 @@ class _Opts(ct.Structure):
 
 class _SweepOpts(ct.Structure):
     _fields_ = [("cluster_fill", ct.c_int), ("giant_class", ct.c_int), ("coarsen_combine", ct.c_int),
-                ("light_streams", ct.c_int)]
+                ("light_streams", ct.c_int), ("table_first_sweep", ct.c_int)]
 
 
 class _RunOpts(ct.Structure):
@@ -320,14 +320,16 @@ class Context:
         self.check(lib().mg_tune_mode(self.h, mode), "mg_tune_mode")
 
     def sweep_options(self, cluster_fill: int = FILL_AUTO, giant_class: int = 0,
-                      coarsen_combine: int = COMBINE_AUTO, light_streams: int = 0):
+                      coarsen_combine: int = COMBINE_AUTO, light_streams: int = 0,
+                      table_first_sweep: bool = False):
         """Sweep and coarsening policy (mg_sweep_options): the cluster-table
         fill (FILL_*), the first degree class (13..18, 0 = default) sent to
         the global-table path, and warp combining of equal keys in the
         coarsening (COMBINE_*), and the number of streams the light degree
-        classes are spread over (1..7, 0 = default 2).  Results do not depend
-        on it."""
-        o = _SweepOpts(cluster_fill, giant_class, coarsen_combine, light_streams)
+        classes are spread over (1..7, 0 = default 2), and whether a level's
+        first sweep uses the table kernels (default: table-free kernels).
+        Results do not depend on it."""
+        o = _SweepOpts(cluster_fill, giant_class, coarsen_combine, light_streams, int(table_first_sweep))
         self.check(lib().mg_sweep_options(self.h, ct.byref(o)), "mg_sweep_options")
 
     def tune_table(self) -> list:

@@ -489,6 +489,7 @@ mg_status mg_coarsen(mg_graph *g, const uint32_t *C, uint32_t *C_dense, mg_graph
         ng->wk = WK_F64;
         ng->mass = g->mass;
         ng->integral = g->integral;
+        ng->sorted_rows = 1;  // coarsened rows come out sorted by neighbour community
     });
     if (st != MG_OK) {
         delete ng;
@@ -627,6 +628,7 @@ mg_status mg_sweep_options(mg_ctx *ctx, const mg_sweep_opts *opts) {
     ctx->mws.cluster_fill = fill;
     ctx->mws.giant_class = gc;
     ctx->mws.coarsen_combine = comb;
+    ctx->mws.first_sweep_kernels = !(opts && opts->table_first_sweep);
     ctx->mws.light_streams =
         opts && opts->light_streams ? opts->light_streams : MoveWorkspace::kDefaultLightStreams;
     return MG_OK;

@@ -19,6 +19,9 @@ struct GraphView {
     const uint32_t *col = nullptr;
     const void *w = nullptr;
     int wk = WK_UNIT;
+    // every row strictly increasing (so no repeated neighbour): generated and
+    // coarsened graphs, and uploaded ones that pass the check
+    bool sorted_rows = false;
 };
 
 // Degree bins of one level.  Schemes: 0 = 10 local-move bins, 1 = 11
@@ -132,6 +135,7 @@ struct MoveWorkspace {
     int giant_class = kFirstHeavyClass + kTiers - 1;
     int cluster_fill = MG_FILL_AUTO;
     int coarsen_combine = MG_COMBINE_AUTO;  // MG_COMBINE_*, read by the coarsening of a run
+    int first_sweep_kernels = 1;            // table-free kernels for a level's first sweep
     // heavy-vertex global tables
     DBuf<uint64_t> h_toff;         // table offset per heavy vertex (H+1)
     DBuf<uint32_t> h_tsize;        // table size per heavy vertex
@@ -174,6 +178,9 @@ struct SweepParams {
     // cluster tables: split fill with warp combining (MG_FILL_SPLIT) instead
     // of the own fill
     int split = 0;
+    // the level's first sweep from the identity assignment with sigma = k
+    // (single-graph runs): every neighbour is its own candidate community
+    int first = 0;
 };
 // split fill only when forced: the own fill measured faster on R-MAT-24 at
 // every level (also against splitting the sweeps where communities repeat)
@@ -285,6 +292,7 @@ struct LevelGraph {
         v.col = col.get();
         v.w = wk == WK_U32 ? (const void *)wi.get() : (const void *)w.get();
         v.wk = wk;
+        v.sorted_rows = true;  // generated and coarsened levels have sorted, deduplicated rows
         return v;
     }
 };

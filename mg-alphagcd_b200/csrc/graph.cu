@@ -185,6 +185,17 @@ __global__ void check_csr_kernel(const uint64_t *off64, uint32_t n, const uint32
     if (b) atomicOr(bad, b);
 }
 
+// *unsorted |= 1 when a row is not strictly increasing (a warp per row)
+__global__ void rows_sorted_kernel(const uint32_t *off, const uint32_t *col, uint32_t n, int *unsorted) {
+    const uint32_t lane = threadIdx.x & 31u;
+    int bad = 0;
+    for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += (gridDim.x * blockDim.x) >> 5) {
+        const uint32_t hi = off[r + 1];
+        for (uint32_t e = off[r] + lane; e + 1 < hi; e += 32) bad |= col[e] >= col[e + 1];
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(unsorted, 1);
+}
+
 // per-block partial sums of weights and integrality flags
 template <class T>
 __global__ void weight_stats_kernel(const T *w, uint64_t m, double *partial, int *nonintegral, int *nonunit) {
@@ -232,6 +243,20 @@ static void device_weight_stats(const T *w, uint64_t m, double &mass, int &integ
     mass = t;
     integral = !hf[0] && t < 4294967296.0;
     unit = !hf[1];
+}
+
+// whether every row of an uploaded graph is strictly increasing
+static int detect_sorted_rows(mg_graph *g, cudaStream_t s) {
+    if (g->n == 0) return 1;
+    DBuf<int> flag;
+    int *d = flag.ensure(1);
+    MG_CUDA(cudaMemsetAsync(d, 0, sizeof(int), s));
+    rows_sorted_kernel<<<148 * 16, 256, 0, s>>>(g->off.get(), g->col.get(), g->n, d);
+    MG_LAUNCH_CHECK();
+    int h = 0;
+    MG_CUDA(cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MG_CUDA(cudaStreamSynchronize(s));
+    return h == 0;
 }
 
 void graph_from_host_csr(mg_graph *g, uint32_t n, const uint64_t *offsets, const uint32_t *cols, const void *w,
@@ -290,6 +315,7 @@ void graph_from_host_csr(mg_graph *g, uint32_t n, const uint64_t *offsets, const
     g->mass = mass;
     g->integral = !nonint && mass < 4294967296.0;
     MG_CUDA(cudaStreamSynchronize(s));
+    g->sorted_rows = detect_sorted_rows(g, s);
 }
 
 void graph_from_device_csr(mg_graph *g, uint32_t n, uint64_t nnz, const uint32_t *d_off, const uint32_t *d_cols,
@@ -322,6 +348,7 @@ void graph_from_device_csr(mg_graph *g, uint32_t n, uint64_t nnz, const uint32_t
         g->integral = integral;
     }
     MG_CUDA(cudaStreamSynchronize(s));
+    g->sorted_rows = detect_sorted_rows(g, s);
 }
 
 void graph_from_level(mg_graph *g, LevelGraph &lv, int integral, double mass) {
@@ -338,6 +365,7 @@ void graph_from_level(mg_graph *g, LevelGraph &lv, int integral, double mass) {
     g->wk = WK_F64;
     g->integral = integral;
     g->mass = mass;
+    g->sorted_rows = 1;  // levels have sorted, deduplicated rows
     MG_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -358,6 +386,7 @@ static void finish_generated(mg_graph *g, uint32_t n, uint64_t m, DBuf<uint32_t>
     g->wk = WK_UNIT;
     g->mass = (double)lv.nnz;
     g->integral = lv.nnz < 4294967296ull;
+    g->sorted_rows = 1;  // sorted, deduplicated pairs
     MG_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -466,6 +495,7 @@ void graph_generate_chunglu(mg_graph *g, uint32_t n, double exponent, double mea
     csr_from_device_pairs(n, m, u.get(), v.get(), lv, ctx->cws, s, dw);
     g->n = n;
     g->nnz = lv.nnz;
+    g->sorted_rows = 1;  // sorted, deduplicated pairs
     std::swap(g->off.p, lv.off.p);
     std::swap(g->off.cap, lv.off.cap);
     std::swap(g->col.p, lv.col.p);

@@ -35,6 +35,7 @@ struct mg_graph {
     int wk = mg::WK_UNIT;
     double mass = 0;
     int integral = 1;
+    int sorted_rows = 0;  // every row strictly increasing (no repeated neighbour)
     mg::GraphView view() const {
         mg::GraphView v;
         v.n = n;
@@ -42,6 +43,7 @@ struct mg_graph {
         v.off = off.get();
         v.col = col.get();
         v.wk = wk;
+        v.sorted_rows = sorted_rows != 0;
         v.w = wk == mg::WK_F32 ? (const void *)w32.get() : wk == mg::WK_F64 ? (const void *)w64.get() : nullptr;
         return v;
     }

@@ -35,6 +35,7 @@ struct LMArgs {
     int integral;
     int agg;             // communities repeat among neighbours: lane-local run combining (table kernels)
     int split;           // cluster tables: split rows over the CTAs, combine in the warp, insert via DSMEM
+    int first;           // the level's first sweep (P = identity, sigma = k): table-free kernels
     SweepAcc *acc;
     // batched sweeps: graph of each vertex, per-graph control word and gain
     // constants, the three assignment buffers, sum_in per vertex, and the
@@ -1143,6 +1144,19 @@ __global__ void __launch_bounds__(kHeavyThreads) heavy_insert_kernel(LMArgs A, c
     uint32_t *keys = tkeys + toff[h];
     double *vals = tvals + toff[h];
     double e_part = 0, s_part = 0;
+    auto ins = [&](uint32_t key, double val) {
+        uint32_t s = hash_range(key, ts);
+        for (uint32_t p = 0; p < ts; p++) {
+            const uint32_t prev = atomicCAS(keys + s, kEmpty, key);
+            if (prev == kEmpty || prev == key) break;
+            s = s + 1 == ts ? 0 : s + 1;
+        }
+        atomicAdd(vals + s, val);
+    };
+    // run combining (A.agg: sweeps where communities repeat), as in the
+    // shared-memory tables: one global atomic per run of equal communities
+    uint32_t rk = kEmpty;
+    double rs = 0;
     for (uint32_t base = lo + threadIdx.x; base < hi; base += kHeavyThreads * BATCH) {
         uint32_t jj[BATCH], cc[BATCH];
         double ww[BATCH];
@@ -1160,17 +1174,17 @@ __global__ void __launch_bounds__(kHeavyThreads) heavy_insert_kernel(LMArgs A, c
             const uint32_t c = cc[b];
             if (c != src) {
                 if (is_candidate<VER>(c, src, up)) {
-                    uint32_t s = hash_range(c, ts);
-                    for (uint32_t p = 0; p < ts; p++) {
-                        uint32_t cur = ((volatile uint32_t *)keys)[s];
-                        if (cur == c) break;
-                        if (cur == kEmpty) {
-                            uint32_t prev = atomicCAS(keys + s, kEmpty, c);
-                            if (prev == kEmpty || prev == c) break;
+                    if (A.agg) {
+                        if (c == rk) {
+                            rs += ww[b];
+                        } else {
+                            if (rk != kEmpty) ins(rk, rs);
+                            rk = c;
+                            rs = ww[b];
                         }
-                        s = s + 1 == ts ? 0 : s + 1;
+                    } else {
+                        ins(c, ww[b]);
                     }
-                    atomicAdd(vals + s, ww[b]);
                 }
             } else if (jj[b] != v) {
                 e_part += ww[b];
@@ -1179,6 +1193,7 @@ __global__ void __launch_bounds__(kHeavyThreads) heavy_insert_kernel(LMArgs A, c
             }
         }
     }
+    if (rk != kEmpty) ins(rk, rs);
     e_part = warp_sum(e_part);
     s_part = warp_sum(s_part);
     if ((threadIdx.x & 31) == 0) {
@@ -1422,9 +1437,208 @@ void launch_light(int shape, int cls, const LMArgs &A, uint32_t off, uint32_t si
     }
 }
 
+// ============================================================================
+// the first sweep of a level (single graph): every community is one vertex
+// (P = identity, sigma = k) and rows hold no repeated neighbour, so every
+// neighbour j != i is a candidate community of its own with k_ic = w_ij and
+// e = 0 -- no table.  The gain is the same FP64 expression with the same
+// operands as the table kernels', so the result is bit-identical.  T lanes
+// per vertex (T <= 32), or BLOCK threads per vertex for long rows.
+// ============================================================================
+constexpr int kFirstU = 4;  // edges in flight per thread
+
+template <int T, int WK, int PREC, int VER>
+__global__ void __launch_bounds__(256) lm_first_kernel(LMArgs A, uint32_t bin_off, uint32_t bin_size) {
+    using G = typename Prec<PREC>::G;
+    const int up = A.up;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t gl = lane & (T - 1);
+    constexpr uint32_t GPW = 32 / T;
+    double sin = 0;
+    unsigned dcnt = 0;
+    const uint32_t gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarp = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t wb = gwarp * GPW; wb < bin_size; wb += nwarp * GPW) {  // warp-uniform
+        const uint32_t idx = wb + lane / T;
+        const bool active = idx < bin_size;
+        uint32_t i = 0, lo = 0, hi = 0;
+        if (active) {
+            i = A.perm[bin_off + idx];
+            const uint2 r = A.rows[bin_off + idx];
+            lo = r.x;
+            hi = r.y;
+        }
+        const double ki = active ? A.k[i] : 0.0;
+        const double a = active ? A.sigma[i] - ki : 0.0;
+        G best = G(0);
+        uint32_t dst = i;
+        double selfw = 0;
+        for (uint32_t e0 = lo + gl; e0 < hi; e0 += T * kFirstU) {
+            uint32_t jj[kFirstU];
+            double ww[kFirstU], sc[kFirstU];
+#pragma unroll
+            for (int u = 0; u < kFirstU; u++) {
+                const uint32_t e = e0 + u * T;
+                jj[u] = e < hi ? __ldcs(A.col + e) : kEmpty;
+                ww[u] = e < hi ? wload<WK>(A.w, e) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kFirstU; u++) sc[u] = jj[u] != kEmpty && jj[u] != i ? A.sigma[jj[u]] : 0.0;
+#pragma unroll
+            for (int u = 0; u < kFirstU; u++) {
+                const uint32_t j = jj[u];
+                if (j == kEmpty) continue;
+                if (j == i) {
+                    selfw += ww[u];
+                    continue;
+                }
+                if (!is_candidate<VER>(j, i, up)) continue;
+                dcnt++;
+                const G gn = Prec<PREC>::gain(ww[u], 0.0, ki, a, sc[u], A.K);
+                if (better(gn, j, best, dst, up)) {
+                    best = gn;
+                    dst = j;
+                }
+            }
+        }
+#pragma unroll
+        for (int o = T / 2; o > 0; o >>= 1) {
+            const G g2 = shfl_xor_g(best, o);
+            const uint32_t c2 = __shfl_xor_sync(0xffffffffu, dst, o);
+            if (better(g2, c2, best, dst, up)) {
+                best = g2;
+                dst = c2;
+            }
+            selfw += __shfl_xor_sync(0xffffffffu, selfw, o);
+        }
+        if (active && gl == 0) {
+            A.N[i] = final_choice<VER>(dst, i, up);
+            sin += selfw;
+        }
+    }
+    flush_acc(A.acc, A.integral, sin, dcnt);
+}
+
+template <int BLOCK, int WK, int PREC, int VER>
+__global__ void __launch_bounds__(BLOCK) lm_first_block_kernel(LMArgs A, uint32_t bin_off, uint32_t bin_size) {
+    using G = typename Prec<PREC>::G;
+    const int up = A.up;
+    __shared__ G red_g[BLOCK / 32];
+    __shared__ uint32_t red_c[BLOCK / 32];
+    __shared__ double red_s[BLOCK / 32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    double sin = 0;
+    unsigned dcnt = 0;
+    for (uint32_t idx = blockIdx.x; idx < bin_size; idx += gridDim.x) {  // uniform over the block
+        const uint32_t i = A.perm[bin_off + idx];
+        const uint2 r = A.rows[bin_off + idx];
+        const uint32_t lo = r.x, hi = r.y;
+        const double ki = A.k[i];
+        const double a = A.sigma[i] - ki;
+        G best = G(0);
+        uint32_t dst = i;
+        double selfw = 0;
+        for (uint32_t e0 = lo + threadIdx.x; e0 < hi; e0 += BLOCK * kFirstU) {
+            uint32_t jj[kFirstU];
+            double ww[kFirstU], sc[kFirstU];
+#pragma unroll
+            for (int u = 0; u < kFirstU; u++) {
+                const uint32_t e = e0 + u * BLOCK;
+                jj[u] = e < hi ? __ldcs(A.col + e) : kEmpty;
+                ww[u] = e < hi ? wload<WK>(A.w, e) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kFirstU; u++) sc[u] = jj[u] != kEmpty && jj[u] != i ? A.sigma[jj[u]] : 0.0;
+#pragma unroll
+            for (int u = 0; u < kFirstU; u++) {
+                const uint32_t j = jj[u];
+                if (j == kEmpty) continue;
+                if (j == i) {
+                    selfw += ww[u];
+                    continue;
+                }
+                if (!is_candidate<VER>(j, i, up)) continue;
+                dcnt++;
+                const G gn = Prec<PREC>::gain(ww[u], 0.0, ki, a, sc[u], A.K);
+                if (better(gn, j, best, dst, up)) {
+                    best = gn;
+                    dst = j;
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const G g2 = shfl_xor_g(best, o);
+            const uint32_t c2 = __shfl_xor_sync(0xffffffffu, dst, o);
+            if (better(g2, c2, best, dst, up)) {
+                best = g2;
+                dst = c2;
+            }
+            selfw += __shfl_xor_sync(0xffffffffu, selfw, o);
+        }
+        if (lane == 0) {
+            red_g[warp] = best;
+            red_c[warp] = dst;
+            red_s[warp] = selfw;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = red_s[0];
+            for (int w2 = 1; w2 < BLOCK / 32; w2++) {
+                if (better(red_g[w2], red_c[w2], best, dst, up)) {
+                    best = red_g[w2];
+                    dst = red_c[w2];
+                }
+                s += red_s[w2];
+            }
+            A.N[i] = final_choice<VER>(dst, i, up);
+            sin += s;
+        }
+        __syncthreads();  // red_* are reused by the next vertex
+    }
+    flush_acc(A.acc, A.integral, sin, dcnt);
+}
+
+template <int WK, int PREC, int VER>
+void launch_first(int cls, const LMArgs &A, uint32_t off, uint32_t size, cudaStream_t s) {
+    if (size == 0) return;
+    auto lanes = [&](auto kern, int T) {
+        const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(size, 256 / T), 148ull * 32);
+        kern<<<grid, 256, 0, s>>>(A, off, size);
+        MG_LAUNCH_CHECK();
+    };
+    auto block = [&](auto kern, int bs) {
+        const unsigned grid = (unsigned)std::min<uint64_t>(size, 148ull * (2048 / bs) * 4);
+        kern<<<grid, bs, 0, s>>>(A, off, size);
+        MG_LAUNCH_CHECK();
+    };
+    if (cls <= 1) lanes(lm_first_kernel<2, WK, PREC, VER>, 2);
+    else if (cls == 2) lanes(lm_first_kernel<4, WK, PREC, VER>, 4);
+    else if (cls == 3) lanes(lm_first_kernel<8, WK, PREC, VER>, 8);
+    else if (cls == 4) lanes(lm_first_kernel<16, WK, PREC, VER>, 16);
+    else if (cls <= 9) lanes(lm_first_kernel<32, WK, PREC, VER>, 32);
+    else if (cls < kFirstHeavyClass) block(lm_first_block_kernel<256, WK, PREC, VER>, 256);
+    else block(lm_first_block_kernel<1024, WK, PREC, VER>, 1024);
+}
+
 template <int WK, int PREC, int VER, int BT>
 void launch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, const LMArgs &A, cudaStream_t s) {
     const Bins &B = lvl.bins;
+    if constexpr (BT == 0) {
+        if (A.first) {
+            // the level's first sweep: no tables (every class, heavy ones included)
+            MG_CUDA(cudaEventRecord(ws.ev_fork, s));
+            const int ns = 1 + std::max(1, std::min(ws.light_streams, MoveWorkspace::kStreams - 1));
+            for (int q = 0; q < ns; q++) MG_CUDA(cudaStreamWaitEvent(ws.streams[q], ws.ev_fork, 0));
+            for (int c = kSweepClasses - 1; c >= 0; c--)
+                launch_first<WK, PREC, VER>(c, A, B.offset[c], B.size[c], ws.streams[c % ns]);
+            for (int q = 0; q < ns; q++) {
+                MG_CUDA(cudaEventRecord(ws.ev_join[q], ws.streams[q]));
+                MG_CUDA(cudaStreamWaitEvent(s, ws.ev_join[q], 0));
+            }
+            return;
+        }
+    }
     // fork: heavy path on its own stream, the light classes on two others
     MG_CUDA(cudaEventRecord(ws.ev_fork, s));
     const int ns = 1 + std::max(1, std::min(ws.light_streams, MoveWorkspace::kStreams - 1));

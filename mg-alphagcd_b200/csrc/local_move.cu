@@ -260,6 +260,7 @@ LMArgs single_args(const GraphView &g, MoveWorkspace &ws, const SweepParams &p, 
     A.integral = p.integral;
     A.agg = p.agg;
     A.split = p.split;
+    A.first = p.first;
     A.acc = ws.acc.ensure(1);
     if (p.precision == MG_PREC_INT64)
         MG_CHECK(p.integral && p.mass < 2147483648.0, MG_ERR_UNSUPPORTED,

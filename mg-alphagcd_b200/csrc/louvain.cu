@@ -140,6 +140,7 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
         sp.up = 1;
         sp.agg = 0;
         sp.split = sweep_split(ctx->mws, 0);
+        sp.first = ctx->mws.first_sweep_kernels && cur.sorted_rows;
         // shapes of the light classes from the tuning table; classes missing
         // from it are timed on the level's second sweep, which is more like
         // the rest of the level than the first (every community one vertex)
@@ -168,6 +169,7 @@ void louvain_run(mg_ctx *ctx, const mg_graph *g, const mg_run_opts &o, mg_result
             sp.up = !sp.up;
             // combine equal communities in the warp once they repeat: fewer
             // than half of the last sweep's edges were distinct candidates
+            sp.first = 0;
             sp.agg = 2 * hacc.distinct < cur.nnz;
             sp.split = sweep_split(ctx->mws, sp.agg);
             const int next = 3 - base - pend;

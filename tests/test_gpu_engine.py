@@ -394,3 +394,27 @@ def test_louvain_combine_modes(O, ctx, combine):
             _compare_runs(_up(ctx, g).louvain(), O.louvain(g))
     finally:
         ctx.sweep_options()
+
+
+def test_first_sweep_kernels_equal_table_kernels(O, ctx):
+    """A level's first sweep (every community one vertex) runs table-free
+    kernels by default; forcing the table kernels gives the same runs, and
+    both equal the oracle (integral weights bit for bit, real weights: the
+    same assignment is not required, Q within 1e-3)."""
+    graphs = [("rmat14", O.gen_rmat(14, seed=2)), ("sbm64k", O.gen_sbm(65536, 64, 16.0, 0.8, seed=1))]
+    try:
+        for name, g in graphs:
+            dg = _up(ctx, g)
+            ref = O.louvain(g)
+            for table_first in (False, True):
+                ctx.sweep_options(table_first_sweep=table_first)
+                for version in (1, 2):
+                    _compare_runs(dg.louvain(version=version), O.louvain(g, version=version) if version == 1 else ref)
+        g = O.gen_chunglu(1 << 15, max_degree=5000.0, seed=3)
+        dg = _up(ctx, g, weights_f32=True)
+        ref = O.louvain(g)
+        for table_first in (False, True):
+            ctx.sweep_options(table_first_sweep=table_first)
+            assert abs(dg.louvain()["modularity"] - ref["modularity"]) <= 1e-3
+    finally:
+        ctx.sweep_options()
