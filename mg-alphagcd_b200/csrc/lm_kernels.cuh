@@ -567,10 +567,14 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
             const uint32_t u0 = ub + lane;
             uint32_t kk[EB];
             double sc[EB], kv[EB];
+            // sub-steps wholly past the candidates are skipped by the warp
+            // (uniform tests: few candidates is the common case once
+            // communities form)
 #pragma unroll
             for (int b = 0; b < EB; b++) {
-                const uint32_t u = u0 + b * GT;
                 kk[b] = kEmpty;
+                if (ub + b * GT >= nd) break;
+                const uint32_t u = u0 + b * GT;
                 if (u < nd) {
                     const uint32_t h = used[u];
                     kk[b] = keys[h];
@@ -580,10 +584,13 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
                 }
             }
 #pragma unroll
-            for (int b = 0; b < EB; b++)
+            for (int b = 0; b < EB; b++) {
+                if (ub + b * GT >= nd) break;
                 if (kk[b] != kEmpty) sc[b] = A.sigma[kk[b]];
+            }
 #pragma unroll
             for (int b = 0; b < EB; b++) {
+                if (ub + b * GT >= nd) break;
                 if (kk[b] != kEmpty) {
                     G gn = Prec<PREC>::gain(kv[b], e_src, ki, a, sc[b], kref<BT>(A, vv));
                     if (better(gn, kk[b], best, dst, up)) {
@@ -1049,10 +1056,12 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
             const uint32_t u0 = ub + (threadIdx.x & 31u);
             uint32_t kk[EB];
             double kv[EB], sc[EB];
+            // sub-steps wholly past the candidates are skipped (uniform tests)
 #pragma unroll
             for (int b = 0; b < EB; b++) {
-                const uint32_t u = u0 + b * kClusterThreads;
                 kk[b] = kEmpty;
+                if (ub + b * kClusterThreads >= nd) break;
+                const uint32_t u = u0 + b * kClusterThreads;
                 if (u < nd) {
                     const uint32_t s = used[u];
                     kk[b] = keys[s];
@@ -1062,10 +1071,13 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
                 }
             }
 #pragma unroll
-            for (int b = 0; b < EB; b++)
+            for (int b = 0; b < EB; b++) {
+                if (ub + b * kClusterThreads >= nd) break;
                 if (kk[b] != kEmpty) sc[b] = A.sigma[kk[b]];
+            }
 #pragma unroll
             for (int b = 0; b < EB; b++) {
+                if (ub + b * kClusterThreads >= nd) break;
                 if (kk[b] != kEmpty) {
                     G gn = Prec<PREC>::gain(kv[b], e_src, ki, a, sc[b], kref<BT>(A, vv));
                     if (better(gn, kk[b], best, dst, up)) {
