@@ -329,6 +329,8 @@ __device__ __forceinline__ void group_sync() {
     else __syncthreads();
 }
 
+// argmax over a group of GT threads; the result is valid in the group's first
+// thread (the only one its callers read it from)
 template <int GT, class G>
 __device__ __forceinline__ void group_argmax(G &best, uint32_t &dst, int up, G *rg, uint32_t *rc) {
 #pragma unroll
@@ -350,11 +352,13 @@ __device__ __forceinline__ void group_argmax(G &best, uint32_t &dst, int up, G *
             rc[warp] = dst;
         }
         __syncthreads();
-#pragma unroll
-        for (int w2 = 0; w2 < GT / 32; w2++) {
-            if (better(rg[w0 + w2], rc[w0 + w2], best, dst, up)) {
-                best = rg[w0 + w2];
-                dst = rc[w0 + w2];
+        if (threadIdx.x % GT == 0) {
+#pragma unroll 8
+            for (int w2 = 1; w2 < GT / 32; w2++) {
+                if (better(rg[w0 + w2], rc[w0 + w2], best, dst, up)) {
+                    best = rg[w0 + w2];
+                    dst = rc[w0 + w2];
+                }
             }
         }
         __syncthreads();
