@@ -491,6 +491,8 @@ def run_batched(mg, ctx, args):
         "sweeps": runs[-1]["sweeps"], "levels": runs[-1]["levels"],
         "gpu_launches": runs[-1]["kernel_launches"],
         "loop_graphs_per_s": k / loop_wall, "loop_sample": k, "loop_device_graphs_per_s": k / loop_dev,
+        "loop_sample_wall_s": loop_wall, "loop_sample_device_s": loop_dev,
+        "loop_extrapolated_wall_s": loop_wall * args.batch_graphs / k,
         "speedup_vs_loop": (args.batch_graphs / wall) / (k / loop_wall),
         "modularity_equal": f"{same}/{k}", "mean_modularity": float(q.mean()),
         "mode": "CUDA-graph iteration loop (MG_BATCH_GRAPHS)",

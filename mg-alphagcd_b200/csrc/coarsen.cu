@@ -384,7 +384,156 @@ uint32_t unique_runs(const uint64_t *keys, size_t m, int bc, uint32_t n_rows, Le
     return u;
 }
 
+// ---- sorted keys -> CSR in two tiled passes (integral weights) -------------
+// A tile of kRunTile sorted keys: each thread takes kRunPer consecutive keys
+// (staged in shared memory); a key starts a run when it differs from the one
+// before it.  Pass 1 counts the runs of every tile; pass 2, given the tiles'
+// run offsets, writes every run's column and first position and the row
+// offsets (a run whose row differs from the previous key's opens that row and
+// every empty row before it).
+constexpr int kRunThreads = 256;
+constexpr int kRunPer = 16;
+constexpr uint32_t kRunTile = kRunThreads * kRunPer;
+
+__global__ void __launch_bounds__(kRunThreads) run_count_kernel(const uint64_t *keys, size_t m, uint32_t *tcount) {
+    __shared__ uint32_t wsum[kRunThreads / 32];
+    const uint32_t t = threadIdx.x;
+    for (size_t tile = blockIdx.x; tile * kRunTile < m; tile += gridDim.x) {
+        const size_t t0 = tile * kRunTile;
+        uint32_t c = 0;
+#pragma unroll 4
+        for (int k = 0; k < kRunPer; k++) {
+            const size_t i = t0 + (size_t)k * kRunThreads + t;  // coalesced; heads need no order here
+            if (i < m) c += (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+        }
+        c = warp_sum(c);
+        if ((t & 31) == 0) wsum[t >> 5] = c;
+        __syncthreads();
+        if (t == 0) {
+            uint32_t s = 0;
+            for (int w = 0; w < kRunThreads / 32; w++) s += wsum[w];
+            tcount[tile] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// rows [r0, r1] of a long gap of empty rows all start at p (filled by
+// fill_gaps_kernel, so that no thread walks millions of empty rows)
+struct RowGap {
+    uint32_t r0, r1, p;
+};
+constexpr uint32_t kInlineRows = 64;
+
+__device__ __forceinline__ void set_rows(uint32_t *off, uint32_t r0, uint32_t r1, uint32_t p, RowGap *gaps,
+                                         uint32_t *ngaps) {
+    if (r0 > r1) return;
+    if (r1 - r0 < kInlineRows) {
+        for (uint32_t r = r0; r <= r1; r++) off[r] = p;
+    } else {
+        gaps[atomicAdd(ngaps, 1u)] = RowGap{r0, r1, p};
+    }
+}
+
+__global__ void fill_gaps_kernel(const RowGap *gaps, const uint32_t *ngaps, uint32_t *off) {
+    const uint32_t ng = *ngaps;
+    for (uint32_t gi = blockIdx.x; gi < ng; gi += gridDim.x) {
+        const RowGap gp = gaps[gi];
+        for (uint32_t r = gp.r0 + threadIdx.x; r <= gp.r1; r += blockDim.x) off[r] = gp.p;
+    }
+}
+
+__global__ void __launch_bounds__(kRunThreads) run_emit_kernel(const uint64_t *keys, size_t m, int bc,
+                                                               uint32_t n_rows, const uint32_t *toff, uint32_t u,
+                                                               uint32_t *col, uint32_t *ustart, uint32_t *off,
+                                                               RowGap *gaps, uint32_t *ngaps) {
+    // logical position x (0: the key before the tile, q + 1: the tile's q-th
+    // key) lives at x + x/16: a thread's 16 consecutive keys then fall on
+    // different banks than its neighbours'
+    __shared__ uint64_t sk[kRunTile + 1 + (kRunTile + 1) / 16 + 1];
+    __shared__ uint32_t wsum[kRunThreads / 32];
+    const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
+    const uint64_t mask = (1ull << bc) - 1ull;
+    for (size_t tile = blockIdx.x; tile * kRunTile < m; tile += gridDim.x) {
+        const size_t t0 = tile * kRunTile;
+        const uint32_t tn = (uint32_t)(m - t0 < kRunTile ? m - t0 : kRunTile);
+        for (uint32_t q = t; q < tn; q += kRunThreads) sk[(q + 1) + ((q + 1) >> 4)] = keys[t0 + q];
+        if (t == 0) sk[0] = t0 ? keys[t0 - 1] : ~0ull;
+        __syncthreads();
+        // this thread's keys: positions [t * kRunPer, (t + 1) * kRunPer) of the tile
+        uint32_t c = 0;
+#pragma unroll
+        for (int k = 0; k < kRunPer; k++) {
+            const uint32_t q = t * kRunPer + k;
+            if (q < tn && ((t0 == 0 && q == 0) || sk[(q + 1) + ((q + 1) >> 4)] != sk[q + (q >> 4)])) c++;
+        }
+        // exclusive prefix of the heads over the tile's threads
+        uint32_t inc = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if ((int)lane >= o) inc += y;
+        }
+        if (lane == 31) wsum[warp] = inc;
+        __syncthreads();
+        uint32_t before = 0;
+        for (uint32_t w = 0; w < warp; w++) before += wsum[w];
+        uint32_t p = toff[tile] + before + inc - c;
+#pragma unroll
+        for (int k = 0; k < kRunPer; k++) {
+            const uint32_t q = t * kRunPer + k;
+            if (q >= tn) break;
+            const uint64_t key = sk[(q + 1) + ((q + 1) >> 4)];
+            const bool first = t0 == 0 && q == 0;
+            const uint64_t prev = sk[q + (q >> 4)];
+            if (!first && key == prev) continue;
+            col[p] = (uint32_t)(key & mask);
+            ustart[p] = (uint32_t)(t0 + q);
+            // rows (previous key's row, this row] start at this run
+            const uint32_t row = (uint32_t)(key >> bc);
+            const uint32_t r0 = first ? 0u : (uint32_t)(prev >> bc) + 1u;
+            set_rows(off, r0, row, p, gaps, ngaps);
+            p++;
+        }
+        // after the last key: the remaining rows (and off[n_rows]) end at u
+        if (t0 + tn == m && tn > 0 && t == (tn - 1) / kRunPer) {
+            set_rows(off, (uint32_t)(sk[tn + (tn >> 4)] >> bc) + 1u, n_rows, u, gaps, ngaps);
+        }
+        __syncthreads();  // sk and wsum are reused by the next tile
+    }
+}
+
 }  // namespace
+
+// Sorted keys -> CSR (off, col) and per-run starts; returns the count.  For
+// callers that need no per-entry run index (integral weights).
+uint32_t unique_runs_tiled(const uint64_t *keys, size_t m, int bc, uint32_t n_rows, LevelGraph &out,
+                           CoarsenWorkspace &ws, cudaStream_t s, uint32_t **ustart_out) {
+    const uint64_t tiles = ceil_div(m, kRunTile);
+    uint32_t *tcount = ws.tcount.ensure(tiles + 1);
+    const unsigned grid = (unsigned)std::min<uint64_t>(tiles, 148ull * 8);
+    run_count_kernel<<<grid, kRunThreads, 0, s>>>(keys, m, tcount);
+    MG_LAUNCH_CHECK();
+    exclusive_scan<uint32_t>(tcount, tcount, tiles, tcount + tiles, s, ws.prim);
+    uint32_t u = 0;
+    MG_CUDA(cudaMemcpyAsync(&u, tcount + tiles, sizeof u, cudaMemcpyDeviceToHost, s));
+    MG_CUDA(cudaStreamSynchronize(s));
+    uint32_t *ustart = ws.u32tmp.ensure((size_t)u + 1);
+    out.n = n_rows;
+    out.nnz = u;
+    uint32_t *off = out.off.ensure((size_t)n_rows + 1);
+    uint32_t *col = out.col.ensure((size_t)u + 1);
+    // at most one gap per run, plus the rows after the last key
+    RowGap *gaps = (RowGap *)ws.u64tmp.ensure(((size_t)u + 2) * sizeof(RowGap) / sizeof(uint64_t) + 2);
+    uint32_t *ngaps = ws.rowcnt.ensure(1);
+    MG_CUDA(cudaMemsetAsync(ngaps, 0, sizeof(uint32_t), s));
+    run_emit_kernel<<<grid, kRunThreads, 0, s>>>(keys, m, bc, n_rows, tcount, u, col, ustart, off, gaps, ngaps);
+    MG_LAUNCH_CHECK();
+    fill_gaps_kernel<<<148 * 8, 256, 0, s>>>(gaps, ngaps, off);
+    MG_LAUNCH_CHECK();
+    *ustart_out = ustart;
+    return u;
+}
 
 void level_weights_f64(const GraphView &g, double *out, cudaStream_t s) {
     if (g.nnz == 0) return;
@@ -494,8 +643,11 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
     else flipped = radix_sort<NoVal>(keys, (NoVal *)nullptr, keys2, (NoVal *)nullptr, mm, 2 * bc, s, ws.prim);
     const uint64_t *sk = flipped ? keys2 : keys;
     const double *sv = flipped ? vals2 : vals;
-    uint32_t *ustart, *seg, *head;
-    uint32_t u = unique_runs(sk, mm, bc, n_new, out, ws, s, &ustart, &seg, &head);
+    uint32_t *ustart, *seg = nullptr, *head = nullptr;
+    // integral weights need only each run's first position; real weights
+    // also the run index of every entry (segmented sums)
+    uint32_t u = integral ? unique_runs_tiled(sk, mm, bc, n_new, out, ws, s, &ustart)
+                          : unique_runs(sk, mm, bc, n_new, out, ws, s, &ustart, &seg, &head);
     if (integral && !weighted) {
         uint32_t *wi = out.wi.ensure(u + 1);  // (allocations stay out of launch argument lists)
         run_lengths_kernel<uint32_t><<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)mm, wi);

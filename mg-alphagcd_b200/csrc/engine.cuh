@@ -58,10 +58,23 @@ struct SweepAcc {
 };
 
 // Heavy vertices (last bin) are split into tiers by degree: tier t < 5 is
-// served by clusters of 2^t CTAs holding one distributed shared-memory table
-// of 2^t * kClusterSlots slots (load <= 1/2); the last tier (giants) by the
-// multi-CTA global-table path.
+// served by clusters of tier_ctas(t) CTAs holding one distributed
+// shared-memory table of tier_ctas(t) segments (load <= 1/2); the last tier
+// (giants) by the multi-CTA global-table path.
 constexpr int kClusterSlots = 16384;
+// Slots of one CTA's table segment.  (22,528 slots of 32-bit sums also fit one
+// CTA, which would serve classes 15-17 with 3, 6 and 12 CTAs instead of 4, 8
+// and 16; measured on R-MAT-24 the run went 0.52 -> 0.69 s: a CTA that needs
+// 226 KB of shared memory waits for an empty SM instead of sharing one with
+// the light-class kernels that run beside it.)
+template <int WK>
+constexpr int kSegSlots = kClusterSlots;
+// CTAs of the cluster serving heavy tier t (degree class 13 + t, degrees up
+// to 2^(13+t)) at table load <= 1/2: 1, 2, 4, 8, 16.
+template <int WK>
+constexpr int tier_ctas(int t) {
+    return (int)((2ull * (1ull << (13 + t)) + kSegSlots<WK> - 1) / kSegSlots<WK>);
+}
 constexpr int kTiers = 6;
 
 // Kernel shapes of the light classes (0-12): T-lane tiles (deg <= T) and

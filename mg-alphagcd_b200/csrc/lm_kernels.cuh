@@ -894,7 +894,7 @@ __global__ void __launch_bounds__(kWarpThreads) lm_warp_kernel(LMArgs A, uint32_
 
 // ============================================================================
 // classes 13-17: one vertex per thread-block cluster of CS CTAs, the
-// cluster's shared memory holding one hash table of CS * kClusterSlots slots.
+// cluster's shared memory holding one hash table of CS * kSegSlots<WK> slots.
 // A neighbour community hashes to (owner CTA, slot); the owner's segment
 // collects its sum (see the two fill modes below), each CTA evaluates the
 // candidates of its segment, and rank 0 reduces the CS winners through
@@ -923,7 +923,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
                                                                         uint32_t count) {
     using G = typename Prec<PREC>::G;
     const int up = load_up<BT>(A);
-    constexpr int S = kClusterSlots;
+    constexpr int S = kSegSlots<WK>;
     constexpr int BATCH = 4;
     constexpr int EB = 4;  // slots per thread per evaluation batch
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -979,7 +979,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
         auto ins = [&](uint32_t key, CV val) {
             const uint32_t h = hash_range(key, (uint32_t)CS * S);
             const unsigned owner = h / S;
-            uint32_t s = h & (S - 1);
+            uint32_t s = h - owner * S;
             uint32_t *ks = owner == rank ? keys : rank_ptr<CS>(keys, owner);
             CV *vs = owner == rank ? vals : rank_ptr<CS>(vals, owner);
             uint16_t *useg = owner == rank ? used : rank_ptr<CS>(used, owner);
@@ -996,7 +996,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
                     placed = true;
                     break;
                 }
-                s = (s + 1) & (S - 1);
+                s = s + 1 == S ? 0 : s + 1;
             }
             if (placed) atomicAdd(vs + s, val);
             else atomicAdd(&A.acc->overflow, 1ull);
@@ -1324,7 +1324,7 @@ __global__ void heavy_final_kernel(LMArgs A, const uint32_t *hv, uint32_t H, con
 
 template <int CS, int WK, int PREC, int VER, int BT>
 size_t cluster_smem() {
-    return (size_t)kClusterSlots * (sizeof(uint32_t) + sizeof(typename ValT<WK>::type) + sizeof(uint16_t));
+    return (size_t)kSegSlots<WK> * (sizeof(uint32_t) + sizeof(typename ValT<WK>::type) + sizeof(uint16_t));
 }
 
 template <int CS, int WK, int PREC, int VER, int BT>
@@ -1663,15 +1663,20 @@ void launch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, c
     const uint32_t *hl = lvl.heavy_list;
     // heavy tiers, largest clusters first
     if (lvl.tier_off[5] > lvl.tier_off[4])
-        launch_cluster<16, WK, PREC, VER, BT>(A, hl + lvl.tier_off[4], lvl.tier_off[5] - lvl.tier_off[4], sh);
+        launch_cluster<tier_ctas<WK>(4), WK, PREC, VER, BT>(A, hl + lvl.tier_off[4], lvl.tier_off[5] - lvl.tier_off[4],
+                                                             sh);
     if (lvl.tier_off[4] > lvl.tier_off[3])
-        launch_cluster<8, WK, PREC, VER, BT>(A, hl + lvl.tier_off[3], lvl.tier_off[4] - lvl.tier_off[3], sh);
+        launch_cluster<tier_ctas<WK>(3), WK, PREC, VER, BT>(A, hl + lvl.tier_off[3], lvl.tier_off[4] - lvl.tier_off[3],
+                                                             sh);
     if (lvl.tier_off[3] > lvl.tier_off[2])
-        launch_cluster<4, WK, PREC, VER, BT>(A, hl + lvl.tier_off[2], lvl.tier_off[3] - lvl.tier_off[2], sh);
+        launch_cluster<tier_ctas<WK>(2), WK, PREC, VER, BT>(A, hl + lvl.tier_off[2], lvl.tier_off[3] - lvl.tier_off[2],
+                                                             sh);
     if (lvl.tier_off[2] > lvl.tier_off[1])
-        launch_cluster<2, WK, PREC, VER, BT>(A, hl + lvl.tier_off[1], lvl.tier_off[2] - lvl.tier_off[1], sh);
+        launch_cluster<tier_ctas<WK>(1), WK, PREC, VER, BT>(A, hl + lvl.tier_off[1], lvl.tier_off[2] - lvl.tier_off[1],
+                                                             sh);
     if (lvl.tier_off[1] > lvl.tier_off[0])
-        launch_cluster<1, WK, PREC, VER, BT>(A, hl + lvl.tier_off[0], lvl.tier_off[1] - lvl.tier_off[0], sm);
+        launch_cluster<tier_ctas<WK>(0), WK, PREC, VER, BT>(A, hl + lvl.tier_off[0], lvl.tier_off[1] - lvl.tier_off[0],
+                                                             sm);
     if (lvl.giants > 0) {
         const uint32_t H = lvl.giants;
         const uint32_t *hv = hl + lvl.tier_off[kTiers - 1];

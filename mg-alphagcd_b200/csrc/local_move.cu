@@ -123,8 +123,10 @@ __global__ void level_init_kernel(const uint32_t *off, const void *w, uint32_t n
 }
 
 // Largest cluster size (8 or 16) the device schedules for the heavy tiers.
+// (the largest tier: 16 CTAs for real weights, 12 for integral ones)
 int probe_max_cluster() {
-    return cluster_capacity<16, WK_F64, MG_PREC_FP64, 2, 0>() > 0 && cluster_capacity<16, WK_UNIT, MG_PREC_FP64, 2, 0>() > 0
+    return cluster_capacity<tier_ctas<WK_F64>(4), WK_F64, MG_PREC_FP64, 2, 0>() > 0 &&
+                   cluster_capacity<tier_ctas<WK_UNIT>(4), WK_UNIT, MG_PREC_FP64, 2, 0>() > 0
                ? 16
                : 8;
 }
@@ -183,10 +185,10 @@ void move_prepare_level(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, c
     for (int t = 0; t <= kTiers; t++) lvl.tier_off[t] = 0;
     if (lvl.heavy == 0) return;
     if (ws.max_cluster == 0) ws.max_cluster = probe_max_cluster();
-    // classes 13..17 are the cluster tiers of 1..16 CTAs (a tier of 2^t CTAs
-    // holds degrees up to 2^t * kClusterSlots / 2), class 18 the giants; on a
-    // device without 16-CTA clusters class 17 joins the giants, and so do the
-    // classes from ws.giant_class on
+    // classes 13..17 are the cluster tiers (tier t: tier_ctas(t) CTAs holding
+    // degrees up to tier_ctas(t) * kSegSlots / 2), class 18 the giants; on a
+    // device without 12- and 16-CTA clusters class 17 joins the giants, and so
+    // do the classes from ws.giant_class on
     int first_giant = std::min(ws.giant_class - kFirstHeavyClass, kTiers - 1);
     if (ws.max_cluster < 16) first_giant = std::min(first_giant, kTiers - 2);
     for (int t = 0; t < kTiers; t++)
