@@ -131,6 +131,15 @@ mg_status mg_graph_generate_chunglu(mg_ctx *ctx, uint32_t n, double exponent, do
 /* n, nnz, mass (sum of all directed weights, src/graph/host_graph.cpp:112-115),
  * integral (1 when every weight is a non-negative integer and mass < 2^32). */
 mg_status mg_graph_info(const mg_graph *g, uint32_t *n, uint64_t *nnz, double *mass, int *integral);
+/* Row properties the engine found (no reference counterpart): sorted_rows = 1
+ * when every row is strictly increasing (generated and coarsened graphs, and
+ * uploads that pass the check: the first sweep of a level then runs
+ * table-free); symmetric = 1 when the weights are integral and the entries
+ * are, as a multiset, their own transposes (generated graphs, their
+ * coarsened levels, and uploads whose two 64-bit fingerprints agree: the
+ * coarsening then sorts only the high half of its keys).  Either pointer may
+ * be NULL. */
+mg_status mg_graph_properties(const mg_graph *g, int *sorted_rows, int *symmetric);
 /* Copy the CSR back to host buffers (offsets[n+1], cols[nnz], weights[nnz]
  * as double; any pointer may be NULL). */
 mg_status mg_graph_copy_csr(const mg_graph *g, uint64_t *offsets, uint32_t *cols, double *weights);

@@ -112,7 +112,7 @@ MG_ERR_TIMEOUT = 7
 EXPORTED = [
     "mg_status_string", "mg_version", "mg_init", "mg_destroy", "mg_last_error", "mg_graph_from_csr",
     "mg_graph_from_device_csr", "mg_graph_from_mtx", "mg_graph_generate_rmat", "mg_graph_generate_sbm",
-    "mg_graph_info", "mg_graph_copy_csr", "mg_graph_destroy", "mg_bins", "mg_bins_offsets", "mg_local_move",
+    "mg_graph_info", "mg_graph_properties", "mg_graph_copy_csr", "mg_graph_destroy", "mg_bins", "mg_bins_offsets", "mg_local_move",
     "mg_modularity", "mg_coarsen", "mg_louvain_run", "mg_result_summary", "mg_result_assignment",
     "mg_result_level_sizes", "mg_result_trace", "mg_result_destroy", "mg_local_move_noalloc",
     "mg_batch_draw_sbm_params", "mg_batch_generate_sbm", "mg_batch_from_csr", "mg_batch_info",
@@ -161,6 +161,7 @@ def lib():
     L.mg_graph_generate_sbm.argtypes = [vp, u32, u32, dbl, dbl, u64, pp]
     L.mg_graph_generate_chunglu.argtypes = [vp, u32, dbl, dbl, dbl, i32, u64, pp]
     L.mg_graph_info.argtypes = [vp, ct.POINTER(u32), ct.POINTER(u64), ct.POINTER(dbl), ct.POINTER(i32)]
+    L.mg_graph_properties.argtypes = [vp, ct.POINTER(i32), ct.POINTER(i32)]
     L.mg_graph_copy_csr.argtypes = [vp, vp, vp, vp]
     L.mg_graph_destroy.argtypes = [vp]
     L.mg_bins.argtypes = [vp, i32, vp, vp, vp, ct.POINTER(u32)]
@@ -634,6 +635,12 @@ class Graph:
         self.ctx.check(lib().mg_graph_info(self.h, ct.byref(n), ct.byref(nnz), ct.byref(mass), ct.byref(integ)),
                        "mg_graph_info")
         return {"n": n.value, "nnz": nnz.value, "mass": mass.value, "integral": bool(integ.value)}
+
+    def properties(self) -> dict:
+        """Row properties found by the engine: sorted rows, symmetric (integral) entries."""
+        so, sy = ct.c_int(), ct.c_int()
+        self.ctx.check(lib().mg_graph_properties(self.h, ct.byref(so), ct.byref(sy)), "mg_graph_properties")
+        return {"sorted_rows": bool(so.value), "symmetric": bool(sy.value)}
 
     @property
     def n(self) -> int:

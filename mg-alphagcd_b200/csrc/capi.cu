@@ -292,6 +292,13 @@ mg_status mg_graph_info(const mg_graph *g, uint32_t *n, uint64_t *nnz, double *m
     return MG_OK;
 }
 
+mg_status mg_graph_properties(const mg_graph *g, int *sorted_rows, int *symmetric) {
+    if (!g) return MG_ERR_INVALID;
+    if (sorted_rows) *sorted_rows = g->sorted_rows;
+    if (symmetric) *symmetric = g->symmetric;
+    return MG_OK;
+}
+
 mg_status mg_graph_copy_csr(const mg_graph *g, uint64_t *offsets, uint32_t *cols, double *weights) {
     if (!g) return MG_ERR_INVALID;
     mg_ctx *ctx = g->ctx;
@@ -490,6 +497,7 @@ mg_status mg_coarsen(mg_graph *g, const uint32_t *C, uint32_t *C_dense, mg_graph
         ng->mass = g->mass;
         ng->integral = g->integral;
         ng->sorted_rows = 1;  // coarsened rows come out sorted by neighbour community
+        ng->symmetric = lv.symmetric;
     });
     if (st != MG_OK) {
         delete ng;

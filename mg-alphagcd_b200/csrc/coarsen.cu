@@ -12,7 +12,9 @@
 // Here every edge becomes a key (C'[u] << b) | C'[v], the keys are radix
 // sorted and equal keys merged, so rows come out sorted by neighbour
 // community.  For integral weights the merged sums are exact (prefix sums
-// over 64-bit integers); for real weights they are double sums.
+// over 64-bit integers); for real weights they are double sums.  A symmetric
+// integral graph is expanded from the transposed side in community order,
+// which leaves only the high half of every key to sort.
 #include <algorithm>
 #include <type_traits>
 
@@ -37,21 +39,28 @@ __global__ void apply_relabel_kernel(const uint32_t *C, uint32_t n, const uint32
 // the non-empty one, wins), a prefix maximum over the tile then gives every
 // edge its row, and the keys are written with coalesced loads and stores.
 // One binary search per tile finds the row holding its first edge.
-// COMBINE: the 32 edges a warp holds at a time are merged by key first (equal
-// keys add their weights, a unit edge counting 1), and only one entry per
-// distinct key is written, to the tile's own region of the output in
-// arrival order; tcount[tile] receives the tile's entry count.  Pays where
-// communities repeat within rows (the end of a phase whose last sweep saw
-// few distinct neighbour communities): the sort then sees far fewer keys.
+// TR (symmetric graphs): the rows are visited in member order -- off holds
+// the offsets of the member-ordered expansion, member r's row starts at
+// msrc[r] of the graph and its community is mcom[r] (non-decreasing in r) --
+// and each entry (v, u) of member v's row is written as the key of its
+// transpose, (C'[u] << bc) | C'[v].  The symmetric graph has the same keys
+// either way, and this order has them sorted by their low half already.
+// COMBINE (never with TR): the 32 edges a warp holds at a time are merged
+// by key first (equal keys add their weights, a unit edge counting 1), and
+// only one entry per distinct key is written, to the tile's own region of
+// the output in arrival order; tcount[tile] receives the tile's entry count.
+// Pays where communities repeat within rows (the end of a phase whose last
+// sweep saw few distinct neighbour communities): the sort then sees far
+// fewer keys.
 constexpr int kExpandThreads = 256;
 constexpr int kExpandPer = 16;
 constexpr uint32_t kExpandTile = kExpandThreads * kExpandPer;
 
-template <int WK, class PV, bool COMBINE = false>
-__global__ void __launch_bounds__(kExpandThreads) expand_keys_kernel(const uint32_t *off, const uint32_t *col,
-                                                                     const void *w, uint32_t n, uint64_t m,
-                                                                     const uint32_t *Cd, int bc, uint64_t *keys,
-                                                                     PV *vals, uint32_t *tcount = nullptr) {
+template <int WK, class PV, bool COMBINE = false, bool TR = false>
+__global__ void __launch_bounds__(kExpandThreads)
+    expand_keys_kernel(const uint32_t *off, const uint32_t *col, const void *w, uint32_t n, uint64_t m,
+                       const uint32_t *Cd, int bc, uint64_t *keys, PV *vals, uint32_t *tcount,
+                       const uint32_t *msrc, const uint32_t *mcom) {
     // tile position q lives at q + q/32 (one padding word per 32: the
     // per-thread runs of 16 positions then fall on distinct banks)
     __shared__ uint32_t rowat[kExpandTile + kExpandTile / 32];
@@ -59,7 +68,19 @@ __global__ void __launch_bounds__(kExpandThreads) expand_keys_kernel(const uint3
     __shared__ uint32_t r0s, tcnt;
     __shared__ PV wstage[COMBINE ? kExpandThreads : 1];
     const uint32_t t = threadIdx.x;
+    static_assert(!(COMBINE && TR), "the member-ordered expansion is not combined");
     if (COMBINE && t == 0) tcnt = 0;
+    // the key and graph position of tile position q (edge e)
+    auto entry = [&](uint32_t q, uint64_t e, uint64_t &key, uint64_t &p) {
+        const uint32_t r = rowat[q + (q >> 5)];
+        if constexpr (TR) {
+            p = msrc[r] + (e - off[r]);
+            key = ((uint64_t)Cd[__ldcs(col + p)] << bc) | mcom[r];
+        } else {
+            p = e;
+            key = ((uint64_t)Cd[r] << bc) | Cd[__ldcs(col + e)];
+        }
+    };
     for (uint64_t E0 = (uint64_t)blockIdx.x * kExpandTile; E0 < m; E0 += (uint64_t)gridDim.x * kExpandTile) {
         const uint64_t E1 = E0 + kExpandTile < m ? E0 + kExpandTile : m;
         if (t == 0) {
@@ -138,10 +159,12 @@ __global__ void __launch_bounds__(kExpandThreads) expand_keys_kernel(const uint3
                 const uint32_t q = k * kExpandThreads + t;
                 const uint64_t e = E0 + q;
                 if (e < E1) {
-                    keys[e] = ((uint64_t)Cd[rowat[q + (q >> 5)]] << bc) | Cd[__ldcs(col + e)];
-                    if constexpr (WK == WK_F32) vals[e] = (PV)__ldcs((const float *)w + e);
-                    else if constexpr (WK == WK_F64) vals[e] = (PV)__ldcs((const double *)w + e);
-                    else if constexpr (WK == WK_U32) vals[e] = (PV)__ldcs((const uint32_t *)w + e);
+                    uint64_t key, p;
+                    entry(q, e, key, p);
+                    keys[e] = key;
+                    if constexpr (WK == WK_F32) vals[e] = (PV)__ldcs((const float *)w + p);
+                    else if constexpr (WK == WK_F64) vals[e] = (PV)__ldcs((const double *)w + p);
+                    else if constexpr (WK == WK_U32) vals[e] = (PV)__ldcs((const uint32_t *)w + p);
                 }
             }
         } else {
@@ -154,11 +177,12 @@ __global__ void __launch_bounds__(kExpandThreads) expand_keys_kernel(const uint3
                 uint64_t key = ~0ull;
                 PV v = PV(0);
                 if (e < E1) {
-                    key = ((uint64_t)Cd[rowat[q + (q >> 5)]] << bc) | Cd[__ldcs(col + e)];
+                    uint64_t p;
+                    entry(q, e, key, p);
                     if constexpr (WK == WK_UNIT) v = PV(1);
-                    else if constexpr (WK == WK_F32) v = (PV)__ldcs((const float *)w + e);
-                    else if constexpr (WK == WK_F64) v = (PV)__ldcs((const double *)w + e);
-                    else v = (PV)__ldcs((const uint32_t *)w + e);
+                    else if constexpr (WK == WK_F32) v = (PV)__ldcs((const float *)w + p);
+                    else if constexpr (WK == WK_F64) v = (PV)__ldcs((const double *)w + p);
+                    else v = (PV)__ldcs((const uint32_t *)w + p);
                 }
                 const uint32_t peers = __match_any_sync(0xffffffffu, key);
                 const bool lead = key != ~0ull && (uint32_t)(__ffs(peers) - 1) == lane;
@@ -207,6 +231,27 @@ __global__ void compact_tiles_kernel(const uint64_t *keys, const PV *vals, const
             okeys[a + i] = keys[src + i];
             ovals[a + i] = vals[src + i];
         }
+    }
+}
+
+// member order of a symmetric coarsening: mkey[v] = (C'[v] << 32) | v, sorted
+// on its community bits, gives the vertices grouped by community
+__global__ void member_keys_kernel(const uint32_t *Cd, uint32_t n, uint64_t *mkey) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        mkey[v] = ((uint64_t)Cd[v] << 32) | v;
+}
+
+// per member r: its row start in the graph, its community, its degree (the
+// exclusive scan of the degrees gives the member-ordered expansion offsets)
+__global__ void member_rows_kernel(const uint64_t *mkey, const uint32_t *off, uint32_t n, uint32_t *msrc,
+                                   uint32_t *mcom, uint32_t *mdeg) {
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const uint64_t k = mkey[r];
+        const uint32_t v = (uint32_t)k;
+        const uint32_t lo = off[v];
+        msrc[r] = lo;
+        mcom[r] = (uint32_t)(k >> 32);
+        mdeg[r] = off[v + 1] - lo;
     }
 }
 
@@ -443,15 +488,25 @@ __global__ void fill_gaps_kernel(const RowGap *gaps, const uint32_t *ngaps, uint
     }
 }
 
+// Pass 2.  A thread holds its 16 keys (and the one before them) in
+// registers; the tile's runs are staged in shared memory (column, first
+// position) and written out with coalesced stores.  LEN (unit weights): also
+// the run lengths, each the distance to the next run's start; the last run
+// of a tile ends in a later tile and gets its length from
+// run_tail_lengths_kernel.
+template <bool LEN>
 __global__ void __launch_bounds__(kRunThreads) run_emit_kernel(const uint64_t *keys, size_t m, int bc,
                                                                uint32_t n_rows, const uint32_t *toff, uint32_t u,
-                                                               uint32_t *col, uint32_t *ustart, uint32_t *off,
-                                                               RowGap *gaps, uint32_t *ngaps) {
+                                                               uint32_t *col, uint32_t *ustart, uint32_t *len,
+                                                               uint32_t *off, RowGap *gaps, uint32_t *ngaps) {
     // logical position x (0: the key before the tile, q + 1: the tile's q-th
     // key) lives at x + x/16: a thread's 16 consecutive keys then fall on
-    // different banks than its neighbours'
-    __shared__ uint64_t sk[kRunTile + 1 + (kRunTile + 1) / 16 + 1];
+    // different banks than its neighbours'.  Reused for the staged runs.
+    constexpr uint32_t kSk = kRunTile + 1 + (kRunTile + 1) / 16 + 1;
+    static_assert(kSk * sizeof(uint64_t) >= 2 * kRunTile * sizeof(uint32_t), "staging fits in the key buffer");
+    __shared__ uint64_t sk[kSk];
     __shared__ uint32_t wsum[kRunThreads / 32];
+    uint32_t *scol = (uint32_t *)sk, *sst = scol + kRunTile;
     const uint32_t t = threadIdx.x, lane = t & 31u, warp = t >> 5;
     const uint64_t mask = (1ull << bc) - 1ull;
     for (size_t tile = blockIdx.x; tile * kRunTile < m; tile += gridDim.x) {
@@ -461,11 +516,17 @@ __global__ void __launch_bounds__(kRunThreads) run_emit_kernel(const uint64_t *k
         if (t == 0) sk[0] = t0 ? keys[t0 - 1] : ~0ull;
         __syncthreads();
         // this thread's keys: positions [t * kRunPer, (t + 1) * kRunPer) of the tile
+        uint64_t kk[kRunPer + 1];
         uint32_t c = 0;
+#pragma unroll
+        for (int k = 0; k <= kRunPer; k++) {
+            const uint32_t x = t * kRunPer + k;  // logical position (key q = x - 1)
+            kk[k] = x <= tn ? sk[x + (x >> 4)] : ~0ull;
+        }
 #pragma unroll
         for (int k = 0; k < kRunPer; k++) {
             const uint32_t q = t * kRunPer + k;
-            if (q < tn && ((t0 == 0 && q == 0) || sk[(q + 1) + ((q + 1) >> 4)] != sk[q + (q >> 4)])) c++;
+            if (q < tn && ((t0 == 0 && q == 0) || kk[k + 1] != kk[k])) c++;
         }
         // exclusive prefix of the heads over the tile's threads
         uint32_t inc = c;
@@ -475,31 +536,54 @@ __global__ void __launch_bounds__(kRunThreads) run_emit_kernel(const uint64_t *k
             if ((int)lane >= o) inc += y;
         }
         if (lane == 31) wsum[warp] = inc;
-        __syncthreads();
-        uint32_t before = 0;
-        for (uint32_t w = 0; w < warp; w++) before += wsum[w];
-        uint32_t p = toff[tile] + before + inc - c;
+        __syncthreads();  // every thread's keys are in registers: sk becomes the staging area
+        uint32_t before = 0, nr = 0;
+        for (uint32_t w = 0; w < kRunThreads / 32; w++) {
+            if (w < warp) before += wsum[w];
+            nr += wsum[w];
+        }
+        const uint32_t base = toff[tile];
+        uint32_t lp = before + inc - c;  // this thread's first run, within the tile
 #pragma unroll
         for (int k = 0; k < kRunPer; k++) {
             const uint32_t q = t * kRunPer + k;
             if (q >= tn) break;
-            const uint64_t key = sk[(q + 1) + ((q + 1) >> 4)];
+            const uint64_t key = kk[k + 1], prev = kk[k];
             const bool first = t0 == 0 && q == 0;
-            const uint64_t prev = sk[q + (q >> 4)];
             if (!first && key == prev) continue;
-            col[p] = (uint32_t)(key & mask);
-            ustart[p] = (uint32_t)(t0 + q);
+            scol[lp] = (uint32_t)(key & mask);
+            sst[lp] = (uint32_t)(t0 + q);
             // rows (previous key's row, this row] start at this run
             const uint32_t row = (uint32_t)(key >> bc);
             const uint32_t r0 = first ? 0u : (uint32_t)(prev >> bc) + 1u;
-            set_rows(off, r0, row, p, gaps, ngaps);
-            p++;
+            set_rows(off, r0, row, base + lp, gaps, ngaps);
+            lp++;
         }
         // after the last key: the remaining rows (and off[n_rows]) end at u
         if (t0 + tn == m && tn > 0 && t == (tn - 1) / kRunPer) {
-            set_rows(off, (uint32_t)(sk[tn + (tn >> 4)] >> bc) + 1u, n_rows, u, gaps, ngaps);
+            set_rows(off, (uint32_t)(keys[t0 + tn - 1] >> bc) + 1u, n_rows, u, gaps, ngaps);
+        }
+        __syncthreads();
+        for (uint32_t i = t; i < nr; i += kRunThreads) {
+            const uint32_t st = sst[i];
+            col[base + i] = scol[i];
+            ustart[base + i] = st;
+            if (LEN && i + 1 < nr) len[base + i] = sst[i + 1] - st;
         }
         __syncthreads();  // sk and wsum are reused by the next tile
+    }
+}
+
+// LEN: the length of each tile's last run, which ends at the next run's start
+// (or at the end of the keys)
+__global__ void run_tail_lengths_kernel(const uint32_t *toff, uint64_t tiles, uint32_t u, uint32_t m,
+                                        const uint32_t *ustart, uint32_t *len) {
+    for (uint64_t tile = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; tile < tiles;
+         tile += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t a = toff[tile], b = toff[tile + 1];
+        if (a == b) continue;  // no run starts in this tile
+        const uint32_t end = b < u ? ustart[b] : m;
+        len[b - 1] = end - ustart[b - 1];
     }
 }
 
@@ -508,7 +592,7 @@ __global__ void __launch_bounds__(kRunThreads) run_emit_kernel(const uint64_t *k
 // Sorted keys -> CSR (off, col) and per-run starts; returns the count.  For
 // callers that need no per-entry run index (integral weights).
 uint32_t unique_runs_tiled(const uint64_t *keys, size_t m, int bc, uint32_t n_rows, LevelGraph &out,
-                           CoarsenWorkspace &ws, cudaStream_t s, uint32_t **ustart_out) {
+                           CoarsenWorkspace &ws, cudaStream_t s, uint32_t **ustart_out, bool lengths) {
     const uint64_t tiles = ceil_div(m, kRunTile);
     uint32_t *tcount = ws.tcount.ensure(tiles + 1);
     const unsigned grid = (unsigned)std::min<uint64_t>(tiles, 148ull * 8);
@@ -527,8 +611,18 @@ uint32_t unique_runs_tiled(const uint64_t *keys, size_t m, int bc, uint32_t n_ro
     RowGap *gaps = (RowGap *)ws.u64tmp.ensure(((size_t)u + 2) * sizeof(RowGap) / sizeof(uint64_t) + 2);
     uint32_t *ngaps = ws.rowcnt.ensure(1);
     MG_CUDA(cudaMemsetAsync(ngaps, 0, sizeof(uint32_t), s));
-    run_emit_kernel<<<grid, kRunThreads, 0, s>>>(keys, m, bc, n_rows, tcount, u, col, ustart, off, gaps, ngaps);
-    MG_LAUNCH_CHECK();
+    if (lengths) {
+        uint32_t *len = out.wi.ensure((size_t)u + 1);
+        run_emit_kernel<true><<<grid, kRunThreads, 0, s>>>(keys, m, bc, n_rows, tcount, u, col, ustart, len, off,
+                                                           gaps, ngaps);
+        MG_LAUNCH_CHECK();
+        run_tail_lengths_kernel<<<grid_for(tiles), 256, 0, s>>>(tcount, tiles, u, (uint32_t)m, ustart, len);
+        MG_LAUNCH_CHECK();
+    } else {
+        run_emit_kernel<false><<<grid, kRunThreads, 0, s>>>(keys, m, bc, n_rows, tcount, u, col, ustart, nullptr,
+                                                            off, gaps, ngaps);
+        MG_LAUNCH_CHECK();
+    }
     fill_gaps_kernel<<<148 * 8, 256, 0, s>>>(gaps, ngaps, off);
     MG_LAUNCH_CHECK();
     *ustart_out = ustart;
@@ -574,6 +668,7 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
     }
     // integral graphs: the next level's weights as exact 32-bit integers
     out.wk = integral ? WK_U32 : WK_F64;
+    out.symmetric = g.symmetric && integral;
     if (m == 0) {
         out.n = n_new;
         out.nnz = 0;
@@ -584,6 +679,32 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
         return;
     }
     if (g.wk == WK_UNIT && !integral) combine = false;  // (a unit graph is always integral)
+    // Symmetric integral graphs: expand from the transposed side in member
+    // order (vertices grouped by community, communities ascending), so the
+    // keys arrive sorted by their low half and the stable sort needs only the
+    // high half's passes; equal keys merge into exact integer sums in any
+    // order, so the CSR is the same as the full sort's.  Not with combining:
+    // the combined keys are few, and the member order costs more than the
+    // passes it saves (R-MAT-24 level 1 -> 2: 17.8 ms full sort, 20.4 ms
+    // member order).
+    const bool tr = g.symmetric && integral && !combine;
+    const uint32_t *msrc = nullptr, *mcom = nullptr, *eoff = g.off;
+    if (tr) {
+        // vertices sorted by community (stable: ascending ids inside one)
+        uint64_t *mk = ws.keys.ensure(std::max<size_t>(m, g.n) + 1);
+        uint64_t *mk2 = ws.keys_alt.ensure(std::max<size_t>(m, g.n) + 1);
+        member_keys_kernel<<<grid_for(g.n), 256, 0, s>>>(Cd, g.n, mk);
+        MG_LAUNCH_CHECK();
+        const bool mf = radix_sort<NoVal>(mk, (NoVal *)nullptr, mk2, (NoVal *)nullptr, g.n, 32 + bc, s, ws.prim, 32);
+        uint32_t *ms = ws.msrc.ensure((size_t)g.n + 1), *mc = ws.mcom.ensure((size_t)g.n + 1);
+        uint32_t *vo = ws.voff.ensure((size_t)g.n + 1);
+        member_rows_kernel<<<grid_for(g.n), 256, 0, s>>>(mf ? mk2 : mk, g.off, g.n, ms, mc, vo);
+        MG_LAUNCH_CHECK();
+        exclusive_scan<uint32_t>(vo, vo, g.n, vo + g.n, s, ws.prim);
+        msrc = ms;
+        mcom = mc;
+        eoff = vo;
+    }
     uint64_t *keys = ws.keys.ensure(m);
     uint64_t *keys2 = ws.keys_alt.ensure(m);
     // combined entries carry their summed weight (unit edges count 1)
@@ -598,29 +719,29 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
     const uint64_t tiles = ceil_div(m, kExpandTile);
     const unsigned gw = grid_for(tiles, 1, 148ull * 8);
     uint32_t *tcount = combine ? ws.tcount.ensure(tiles + 1) : nullptr;
-    auto expand = [&](auto *pv, auto comb) {
+    auto expand = [&](auto *pv, auto comb, auto trv) {
         using PV = typename std::remove_pointer<decltype(pv)>::type;
-        constexpr bool CB = decltype(comb)::value;
+        constexpr bool CB = decltype(comb)::value, TR = decltype(trv)::value;
         if (g.wk == WK_UNIT)
-            expand_keys_kernel<WK_UNIT, PV, CB><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys,
-                                                                               pv, tcount);
+            expand_keys_kernel<WK_UNIT, PV, CB, TR><<<gw, kExpandThreads, 0, s>>>(eoff, g.col, g.w, g.n, m, Cd, bc,
+                                                                                   keys, pv, tcount, msrc, mcom);
         else if (g.wk == WK_F32)
-            expand_keys_kernel<WK_F32, PV, CB><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys,
-                                                                              pv, tcount);
+            expand_keys_kernel<WK_F32, PV, CB, TR><<<gw, kExpandThreads, 0, s>>>(eoff, g.col, g.w, g.n, m, Cd, bc,
+                                                                                  keys, pv, tcount, msrc, mcom);
         else if (g.wk == WK_U32)
-            expand_keys_kernel<WK_U32, PV, CB><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys,
-                                                                              pv, tcount);
+            expand_keys_kernel<WK_U32, PV, CB, TR><<<gw, kExpandThreads, 0, s>>>(eoff, g.col, g.w, g.n, m, Cd, bc,
+                                                                                  keys, pv, tcount, msrc, mcom);
         else
-            expand_keys_kernel<WK_F64, PV, CB><<<gw, kExpandThreads, 0, s>>>(g.off, g.col, g.w, g.n, m, Cd, bc, keys,
-                                                                              pv, tcount);
+            expand_keys_kernel<WK_F64, PV, CB, TR><<<gw, kExpandThreads, 0, s>>>(eoff, g.col, g.w, g.n, m, Cd, bc,
+                                                                                  keys, pv, tcount, msrc, mcom);
         MG_LAUNCH_CHECK();
     };
     // the sort's input: every edge (mm = m), or the combined entries gathered
     // densely into the alternate buffers (mm = their count)
     size_t mm = m;
     if (combine) {
-        if (ipay) expand(ivals, std::true_type());
-        else expand(vals, std::true_type());
+        if (ipay) expand(ivals, std::true_type(), std::false_type());
+        else expand(vals, std::true_type(), std::false_type());
         exclusive_scan<uint32_t>(tcount, tcount, tiles, tcount + tiles, s, ws.prim);
         uint32_t d = 0;
         MG_CUDA(cudaMemcpyAsync(&d, tcount + tiles, sizeof d, cudaMemcpyDeviceToHost, s));
@@ -634,24 +755,27 @@ void coarsen_level(const GraphView &g, const uint32_t *Cd, uint32_t n_new, int i
         std::swap(ivals, ivals2);
         mm = d;
     } else {
-        if (ipay) expand(ivals, std::false_type());
-        else expand(vals, std::false_type());
+        if (tr && ipay) expand(ivals, std::false_type(), std::true_type());
+        else if (tr) expand(vals, std::false_type(), std::true_type());
+        else if (ipay) expand(ivals, std::false_type(), std::false_type());
+        else expand(vals, std::false_type(), std::false_type());
     }
+    // the member-ordered expansion is sorted by the low half already
+    const int lo = tr ? bc : 0;
     bool flipped;
-    if (ipay) flipped = radix_sort<uint32_t>(keys, ivals, keys2, ivals2, mm, 2 * bc, s, ws.prim);
-    else if (weighted) flipped = radix_sort<double>(keys, vals, keys2, vals2, mm, 2 * bc, s, ws.prim);
-    else flipped = radix_sort<NoVal>(keys, (NoVal *)nullptr, keys2, (NoVal *)nullptr, mm, 2 * bc, s, ws.prim);
+    if (ipay) flipped = radix_sort<uint32_t>(keys, ivals, keys2, ivals2, mm, 2 * bc, s, ws.prim, lo);
+    else if (weighted) flipped = radix_sort<double>(keys, vals, keys2, vals2, mm, 2 * bc, s, ws.prim, lo);
+    else flipped = radix_sort<NoVal>(keys, (NoVal *)nullptr, keys2, (NoVal *)nullptr, mm, 2 * bc, s, ws.prim, lo);
     const uint64_t *sk = flipped ? keys2 : keys;
     const double *sv = flipped ? vals2 : vals;
     uint32_t *ustart, *seg = nullptr, *head = nullptr;
     // integral weights need only each run's first position; real weights
     // also the run index of every entry (segmented sums)
-    uint32_t u = integral ? unique_runs_tiled(sk, mm, bc, n_new, out, ws, s, &ustart)
+    // (unit weights of an integral graph: the run lengths come with the runs)
+    uint32_t u = integral ? unique_runs_tiled(sk, mm, bc, n_new, out, ws, s, &ustart, !weighted)
                           : unique_runs(sk, mm, bc, n_new, out, ws, s, &ustart, &seg, &head);
     if (integral && !weighted) {
-        uint32_t *wi = out.wi.ensure(u + 1);  // (allocations stay out of launch argument lists)
-        run_lengths_kernel<uint32_t><<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)mm, wi);
-        MG_LAUNCH_CHECK();
+        // weights written by unique_runs_tiled
     } else if (!weighted) {
         double *w = out.w.ensure(u + 1);
         run_lengths_kernel<double><<<grid_for(u), 256, 0, s>>>(ustart, u, (uint32_t)mm, w);

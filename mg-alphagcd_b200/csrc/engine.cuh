@@ -22,6 +22,11 @@ struct GraphView {
     // every row strictly increasing (so no repeated neighbour): generated and
     // coarsened graphs, and uploaded ones that pass the check
     bool sorted_rows = false;
+    // integral weights and every entry (u, v, w) matched by an entry (v, u, w)
+    // (as multisets): generated graphs, their coarsened levels, and uploaded
+    // integral graphs whose fingerprint check passes.  The coarsening then
+    // expands every edge from its transposed side (see coarsen_level).
+    bool symmetric = false;
 };
 
 // Degree bins of one level.  Schemes: 0 = 10 local-move bins, 1 = 11
@@ -286,6 +291,10 @@ struct CoarsenWorkspace {
     DBuf<uint64_t> u64tmp;
     DBuf<uint32_t> u32tmp;
     DBuf<uint32_t> tcount;  // combined entries per expansion tile
+    // member order of a symmetric coarsening: per member (vertices sorted by
+    // community) its row start, its community, and its row's offset in the
+    // member-ordered expansion
+    DBuf<uint32_t> msrc, mcom, voff;
     PrimWorkspace prim;
 };
 // A device CSR level: f64 weights (w, wk = WK_F64), or exact 32-bit integer
@@ -297,6 +306,7 @@ struct LevelGraph {
     DBuf<double> w;
     DBuf<uint32_t> wi;
     int wk = WK_F64;
+    bool symmetric = false;  // coarsened from a symmetric integral graph
     GraphView view() const {
         GraphView v;
         v.n = n;
@@ -306,6 +316,7 @@ struct LevelGraph {
         v.w = wk == WK_U32 ? (const void *)wi.get() : (const void *)w.get();
         v.wk = wk;
         v.sorted_rows = true;  // generated and coarsened levels have sorted, deduplicated rows
+        v.symmetric = symmetric;
         return v;
     }
 };

@@ -185,15 +185,60 @@ __global__ void check_csr_kernel(const uint64_t *off64, uint32_t n, const uint32
     if (b) atomicOr(bad, b);
 }
 
-// *unsorted |= 1 when a row is not strictly increasing (a warp per row)
-__global__ void rows_sorted_kernel(const uint32_t *off, const uint32_t *col, uint32_t n, int *unsorted) {
+// 64-bit finaliser of SplitMix64 (Steele, Lea and Flood, OOPSLA 2014)
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+// hash of the entry (a, b) with integer weight x under one of two seeds
+__device__ __forceinline__ uint64_t entry_hash(uint32_t a, uint32_t b, uint64_t x, uint64_t seed) {
+    return mix64(mix64((((uint64_t)a << 32) | b) ^ seed) + x * 0x9e3779b97f4a7c15ull);
+}
+
+// A warp per row.  *unsorted |= 1 when a row is not strictly increasing.
+// FP (integral weights): fp[0..3] += the sums over the entries (u, v, x) of
+// h1(u, v, x), h1(v, u, x), h2(u, v, x), h2(v, u, x) (mod 2^64).  A graph
+// whose entries are, as a multiset, their own transposes gives fp[0] ==
+// fp[1] and fp[2] == fp[3]; any other graph gives two equal pairs only by a
+// collision of two independent 64-bit sums.
+template <int WK, bool FP>
+__global__ void row_checks_kernel(const uint32_t *off, const uint32_t *col, const void *w, uint32_t n,
+                                  int *unsorted, unsigned long long *fp) {
+    constexpr uint64_t kSeed1 = 0x243f6a8885a308d3ull, kSeed2 = 0x13198a2e03707344ull;
     const uint32_t lane = threadIdx.x & 31u;
     int bad = 0;
+    uint64_t f0 = 0, f1 = 0, f2 = 0, f3 = 0;
     for (uint32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += (gridDim.x * blockDim.x) >> 5) {
-        const uint32_t hi = off[r + 1];
-        for (uint32_t e = off[r] + lane; e + 1 < hi; e += 32) bad |= col[e] >= col[e + 1];
+        const uint32_t lo = off[r], hi = off[r + 1];
+        for (uint32_t e = lo + lane; e < hi; e += 32) {
+            const uint32_t v = col[e];
+            if (e + 1 < hi) bad |= v >= col[e + 1];
+            if constexpr (FP) {
+                uint64_t x = 1;
+                if constexpr (WK == WK_F32) x = (uint64_t)((const float *)w)[e];
+                else if constexpr (WK == WK_F64) x = (uint64_t)((const double *)w)[e];
+                f0 += entry_hash(r, v, x, kSeed1);
+                f1 += entry_hash(v, r, x, kSeed1);
+                f2 += entry_hash(r, v, x, kSeed2);
+                f3 += entry_hash(v, r, x, kSeed2);
+            }
+        }
     }
     if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(unsorted, 1);
+    if constexpr (FP) {
+        f0 = warp_sum((unsigned long long)f0);
+        f1 = warp_sum((unsigned long long)f1);
+        f2 = warp_sum((unsigned long long)f2);
+        f3 = warp_sum((unsigned long long)f3);
+        if (lane == 0) {
+            atomicAdd(fp + 0, (unsigned long long)f0);
+            atomicAdd(fp + 1, (unsigned long long)f1);
+            atomicAdd(fp + 2, (unsigned long long)f2);
+            atomicAdd(fp + 3, (unsigned long long)f3);
+        }
+    }
 }
 
 // per-block partial sums of weights and integrality flags
@@ -245,18 +290,31 @@ static void device_weight_stats(const T *w, uint64_t m, double &mass, int &integ
     unit = !hf[1];
 }
 
-// whether every row of an uploaded graph is strictly increasing
-static int detect_sorted_rows(mg_graph *g, cudaStream_t s) {
-    if (g->n == 0) return 1;
-    DBuf<int> flag;
-    int *d = flag.ensure(1);
-    MG_CUDA(cudaMemsetAsync(d, 0, sizeof(int), s));
-    rows_sorted_kernel<<<148 * 16, 256, 0, s>>>(g->off.get(), g->col.get(), g->n, d);
-    MG_LAUNCH_CHECK();
-    int h = 0;
-    MG_CUDA(cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, s));
+// An uploaded graph's row properties, in one pass over its entries: whether
+// every row is strictly increasing, and (integral weights) whether it is
+// symmetric as a multiset of entries (fingerprint above).
+static void detect_row_properties(mg_graph *g, cudaStream_t s) {
+    g->sorted_rows = 1;
+    g->symmetric = g->integral;
+    if (g->n == 0) return;
+    DBuf<unsigned long long> flags;
+    unsigned long long *d = flags.ensure(5);
+    MG_CUDA(cudaMemsetAsync(d, 0, 5 * sizeof(unsigned long long), s));
+    int *uns = (int *)(d + 4);
+    const void *w = g->wk == WK_F32 ? (const void *)g->w32.get() : (const void *)g->w64.get();
+    auto run = [&](auto kern) {
+        kern<<<148 * 16, 256, 0, s>>>(g->off.get(), g->col.get(), w, g->n, uns, d);
+        MG_LAUNCH_CHECK();
+    };
+    if (!g->integral) run(row_checks_kernel<WK_UNIT, false>);
+    else if (g->wk == WK_F32) run(row_checks_kernel<WK_F32, true>);
+    else if (g->wk == WK_F64) run(row_checks_kernel<WK_F64, true>);
+    else run(row_checks_kernel<WK_UNIT, true>);
+    unsigned long long h[5];
+    MG_CUDA(cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, s));
     MG_CUDA(cudaStreamSynchronize(s));
-    return h == 0;
+    g->sorted_rows = *(const int *)(h + 4) == 0;
+    g->symmetric = g->integral && h[0] == h[1] && h[2] == h[3];
 }
 
 void graph_from_host_csr(mg_graph *g, uint32_t n, const uint64_t *offsets, const uint32_t *cols, const void *w,
@@ -315,7 +373,7 @@ void graph_from_host_csr(mg_graph *g, uint32_t n, const uint64_t *offsets, const
     g->mass = mass;
     g->integral = !nonint && mass < 4294967296.0;
     MG_CUDA(cudaStreamSynchronize(s));
-    g->sorted_rows = detect_sorted_rows(g, s);
+    detect_row_properties(g, s);
 }
 
 void graph_from_device_csr(mg_graph *g, uint32_t n, uint64_t nnz, const uint32_t *d_off, const uint32_t *d_cols,
@@ -348,7 +406,7 @@ void graph_from_device_csr(mg_graph *g, uint32_t n, uint64_t nnz, const uint32_t
         g->integral = integral;
     }
     MG_CUDA(cudaStreamSynchronize(s));
-    g->sorted_rows = detect_sorted_rows(g, s);
+    detect_row_properties(g, s);
 }
 
 void graph_from_level(mg_graph *g, LevelGraph &lv, int integral, double mass) {
@@ -366,6 +424,7 @@ void graph_from_level(mg_graph *g, LevelGraph &lv, int integral, double mass) {
     g->integral = integral;
     g->mass = mass;
     g->sorted_rows = 1;  // levels have sorted, deduplicated rows
+    g->symmetric = lv.symmetric && integral;
     MG_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -387,6 +446,7 @@ static void finish_generated(mg_graph *g, uint32_t n, uint64_t m, DBuf<uint32_t>
     g->mass = (double)lv.nnz;
     g->integral = lv.nnz < 4294967296ull;
     g->sorted_rows = 1;  // sorted, deduplicated pairs
+    g->symmetric = g->integral;  // both directions of every pair
     MG_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -516,6 +576,7 @@ void graph_generate_chunglu(mg_graph *g, uint32_t n, double exponent, double mea
         device_weight_stats<float>(g->w32.get(), lv.nnz, g->mass, integral, unit, s);
         g->integral = integral;
     }
+    g->symmetric = g->integral;  // both directions of every pair, with its weight
     MG_CUDA(cudaStreamSynchronize(s));
 }
 

@@ -36,6 +36,7 @@ struct mg_graph {
     double mass = 0;
     int integral = 1;
     int sorted_rows = 0;  // every row strictly increasing (no repeated neighbour)
+    int symmetric = 0;    // integral and symmetric as a multiset of entries (GraphView::symmetric)
     mg::GraphView view() const {
         mg::GraphView v;
         v.n = n;
@@ -44,6 +45,7 @@ struct mg_graph {
         v.col = col.get();
         v.wk = wk;
         v.sorted_rows = sorted_rows != 0;
+        v.symmetric = symmetric != 0;
         v.w = wk == mg::WK_F32 ? (const void *)w32.get() : wk == mg::WK_F64 ? (const void *)w64.get() : nullptr;
         return v;
     }

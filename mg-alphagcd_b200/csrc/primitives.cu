@@ -225,8 +225,8 @@ __global__ void __launch_bounds__(kRsThreads) rs_scatter_kernel(const uint64_t *
 
 template <class V>
 bool radix_sort(uint64_t *keys, V *vals, uint64_t *keys_alt, V *vals_alt, size_t n, int bits,
-                cudaStream_t s, PrimWorkspace &ws) {
-    if (n <= 1 || bits <= 0) return false;
+                cudaStream_t s, PrimWorkspace &ws, int lo_bit) {
+    if (n <= 1 || bits <= lo_bit) return false;
     MG_CHECK(n < 0xFFFFFFFFull, MG_ERR_UNSUPPORTED, "radix_sort: more than 2^32-1 keys");
     uint32_t tiles = (uint32_t)ceil_div(n, kRsTile);
     uint32_t *hist = ws.hist.ensure((size_t)tiles * 256 + 1);
@@ -235,7 +235,7 @@ bool radix_sort(uint64_t *keys, V *vals, uint64_t *keys_alt, V *vals_alt, size_t
     bool flipped = false;
     const size_t smem = (size_t)kRsTile * (sizeof(uint64_t) + (std::is_same<V, NoVal>::value ? 0 : sizeof(V)));
     MG_CUDA(cudaFuncSetAttribute(rs_scatter_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    for (int shift = 0; shift < bits; shift += 8) {
+    for (int shift = lo_bit; shift < bits; shift += 8) {
         rs_hist_kernel<<<tiles, kRsThreads, 0, s>>>(ka, n, shift, hist, tiles);
         MG_LAUNCH_CHECK();
         exclusive_scan<uint32_t>(hist, hist, (size_t)tiles * 256, nullptr, s, ws);
@@ -248,10 +248,11 @@ bool radix_sort(uint64_t *keys, V *vals, uint64_t *keys_alt, V *vals_alt, size_t
     return flipped;
 }
 
-template bool radix_sort<NoVal>(uint64_t *, NoVal *, uint64_t *, NoVal *, size_t, int, cudaStream_t, PrimWorkspace &);
+template bool radix_sort<NoVal>(uint64_t *, NoVal *, uint64_t *, NoVal *, size_t, int, cudaStream_t, PrimWorkspace &,
+                                int);
 template bool radix_sort<uint32_t>(uint64_t *, uint32_t *, uint64_t *, uint32_t *, size_t, int, cudaStream_t,
-                                   PrimWorkspace &);
+                                   PrimWorkspace &, int);
 template bool radix_sort<double>(uint64_t *, double *, uint64_t *, double *, size_t, int, cudaStream_t,
-                                 PrimWorkspace &);
+                                 PrimWorkspace &, int);
 
 }  // namespace mg

@@ -25,13 +25,14 @@ struct PrimWorkspace {
 template <class T>
 void exclusive_scan(const T *in, T *out, size_t n, T *d_total, cudaStream_t s, PrimWorkspace &ws);
 
-// Stable LSD radix sort of keys[0,n) on bits [0, bits) (bits <= 64), with
-// an optional payload.  keys/vals and keys_alt/vals_alt are ping-pong
-// buffers of n entries; returns true when the result ended in the *_alt
-// buffers.  V: NoVal, uint32_t or double.
+// Stable LSD radix sort of keys[0,n) on bits [lo_bit, bits) (bits <= 64),
+// with an optional payload: keys equal on those bits keep their input order.
+// keys/vals and keys_alt/vals_alt are ping-pong buffers of n entries; returns
+// true when the result ended in the *_alt buffers.  V: NoVal, uint32_t or
+// double.
 template <class V>
 bool radix_sort(uint64_t *keys, V *vals, uint64_t *keys_alt, V *vals_alt, size_t n, int bits,
-                cudaStream_t s, PrimWorkspace &ws);
+                cudaStream_t s, PrimWorkspace &ws, int lo_bit = 0);
 
 // Number of bits needed to represent values < n (at least 1).
 inline int bits_for(uint64_t n) {
