@@ -204,19 +204,22 @@ def peaks():
         return 6650.0, "fallback"
 
 
-TRAFFIC_PROFILE = "local_move_first_sweep_traffic"
+TRAFFIC_PROFILE = "local_move_level0_sweep_traffic"
 
 
 def traffic_per_sweep():
-    """DRAM bytes of the first level-0 sweep of R-MAT-24 from the committed
-    ncu summary (measured on a smaller R-MAT and scaled by the entry count),
-    the algorithmic bytes of that sweep, and where the figure comes from."""
+    """DRAM bytes of one level-0 table sweep of R-MAT-24 (the second sweep)
+    from the committed ncu summary (measured on smaller R-MATs and scaled by
+    the entry count), the algorithmic bytes bound of that sweep, and where the
+    figures come from."""
     try:
         with open(os.path.join(ROOT, "profiles", TRAFFIC_PROFILE + ".json")) as f:
             p = json.load(f)
-        src = {"profile": p["key"], "measured_at_commit": p["measured_at_commit"], "scaling": p["scaling"],
-               "captures": {k: {"dram_bytes": v["dram_bytes"], "ratio": v["ratio"]} for k, v in p["captures"].items()}}
-        return p["rmat24_dram_bytes_scaled"], p["rmat24_algorithmic_bytes"], src
+        src = {"profile": p["key"], "measured_at_commit": p["measured_at_commit"], "sweep": p["sweep"],
+               "scaling": p["scaling"],
+               "captures": {k: {"dram_bytes": v["dram_bytes"], "first_sweep_dram_bytes": v["first_sweep_dram_bytes"]}
+                            for k, v in p["captures"].items()}}
+        return p["rmat24_dram_bytes_scaled"], p["rmat24_algorithmic_bytes_bound"], src
     except (OSError, ValueError, KeyError):
         return None, None, None
 
@@ -667,7 +670,8 @@ def run_engine(args, world, rank, local, pg):
         "local_move_s": last["seconds_local_move"], "coarsen_s": last["seconds_coarsen"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "traffic_sweep": "first level-0 sweep", "traffic_sweep_algorithmic_bytes": traffic_alg,
+                     "traffic_sweep": traffic_src["sweep"] if traffic_src else None,
+                     "traffic_sweep_algorithmic_bytes_bound": traffic_alg,
                      "traffic_source": traffic_src,
                      "kernel": "local-move sweep (all bins)", "peak_kind": peak_kind,
                      "sweeps": sweeps, "algorithmic_bytes_per_sweep": sweep_b / max(sweeps, 1)},
