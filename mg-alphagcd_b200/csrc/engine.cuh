@@ -67,18 +67,32 @@ struct SweepAcc {
 // shared-memory table of tier_ctas(t) segments (load <= 1/2); the last tier
 // (giants) by the multi-CTA global-table path.
 constexpr int kClusterSlots = 16384;
-// Slots of one CTA's table segment.  (22,528 slots of 32-bit sums also fit one
-// CTA, which would serve classes 15-17 with 3, 6 and 12 CTAs instead of 4, 8
-// and 16; measured on R-MAT-24 the run went 0.52 -> 0.69 s: a CTA that needs
-// 226 KB of shared memory waits for an empty SM instead of sharing one with
-// the light-class kernels that run beside it.)
+// Slots of one CTA's listed table segment.  (22,528 listed slots of 32-bit
+// sums also fit one CTA, which would serve classes 15-17 with 3, 6 and 12
+// CTAs instead of 4, 8 and 16; measured on R-MAT-24 the run went 0.52 ->
+// 0.69 s.  The dense segments below keep power-of-two clusters and 192 KB.)
 template <int WK>
 constexpr int kSegSlots = kClusterSlots;
+// Dense segments (integral weights, tiers 1-4): 24,576 slots of a 32-bit key
+// and a 32-bit sum (192 KB) and no insertion list -- the evaluation scans the
+// slots -- at table load <= 2/3, so one CTA holds 16,384 distinct communities
+// and the tiers need half the CTAs (every CTA of a cluster reads the whole
+// row with the own fill).  Tier 0 (degrees <= 8,192) keeps the list, which
+// spares its short rows a scan of the whole segment.
+constexpr int kDenseSlots = 24576;
+constexpr int kDenseCapacity = kDenseSlots / 3 * 2;
+template <int WK>
+constexpr bool kDenseTier(int t) {
+    return kIntg<WK> && t >= 1;
+}
 // CTAs of the cluster serving heavy tier t (degree class 13 + t, degrees up
-// to 2^(13+t)) at table load <= 1/2: 1, 2, 4, 8, 16.
+// to 2^(13+t)): 1, 2, 4, 8, 16 at table load <= 1/2 with the listed segments,
+// 1, 1, 2, 4, 8 with dense segments.
 template <int WK>
 constexpr int tier_ctas(int t) {
-    return (int)((2ull * (1ull << (13 + t)) + kSegSlots<WK> - 1) / kSegSlots<WK>);
+    return kDenseTier<WK>(t)
+               ? (int)(((1ull << (13 + t)) + kDenseCapacity - 1) / kDenseCapacity)
+               : (int)((2ull * (1ull << (13 + t)) + kSegSlots<WK> - 1) / kSegSlots<WK>);
 }
 constexpr int kTiers = 6;
 

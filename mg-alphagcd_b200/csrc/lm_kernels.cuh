@@ -918,16 +918,18 @@ __device__ __forceinline__ T *rank_ptr(T *p, unsigned r) {
     else return cg::this_cluster().map_shared_rank(p, r);
 }
 
-template <int CS, int WK, int PREC, int VER, int BT>
+template <int CS, int WK, int PREC, int VER, int BT, bool DENSE = false>
 __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A, const uint32_t *verts,
                                                                         uint32_t count) {
     using G = typename Prec<PREC>::G;
     const int up = load_up<BT>(A);
-    constexpr int S = kSegSlots<WK>;
+    static_assert(!DENSE || kIntg<WK>, "dense segments hold 32-bit sums");
+    constexpr int S = DENSE ? kDenseSlots : kSegSlots<WK>;
     constexpr int BATCH = 4;
     constexpr int EB = 4;  // slots per thread per evaluation batch
     extern __shared__ __align__(16) unsigned char smem_raw[];
     // keys u32 [S] | sums [S] (u32 for integral weights, else double) | used u16 [S]
+    // (DENSE: no insertion list; the evaluation scans the segment)
     using CV = typename ValT<WK>::type;
     uint32_t *keys = (uint32_t *)smem_raw;
     CV *vals = (CV *)(smem_raw + sizeof(uint32_t) * S);
@@ -988,7 +990,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
             for (int p = 0; p < S; p++) {
                 const uint32_t prev = atomicCAS(ks + s, kEmpty, key);
                 if (prev == kEmpty) {
-                    useg[atomicAdd(uc, 1u)] = (uint16_t)s;
+                    if constexpr (!DENSE) useg[atomicAdd(uc, 1u)] = (uint16_t)s;
                     placed = true;
                     break;
                 }
@@ -1056,7 +1058,41 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
         G best = G(0);
         uint32_t dst = src;
         const uint32_t nd = ucnt;
-        for (uint32_t ub = threadIdx.x & ~31u; ub < nd; ub += kClusterThreads * EB) {  // warp-uniform
+        if constexpr (DENSE) {
+            // every slot of the segment, EB per thread per step (S is a
+            // multiple of kClusterThreads * EB); the non-empty ones are this
+            // CTA's candidates, reset as they are read
+            static_assert(S % (kClusterThreads * EB) == 0, "whole evaluation steps");
+            for (uint32_t sb = threadIdx.x; sb < (uint32_t)S; sb += kClusterThreads * EB) {
+                uint32_t kk[EB];
+                double kv[EB], sc[EB];
+#pragma unroll
+                for (int b = 0; b < EB; b++) {
+                    const uint32_t s = sb + b * kClusterThreads;
+                    kk[b] = keys[s];
+                    if (kk[b] != kEmpty) {
+                        kv[b] = v2d(vals[s]);
+                        keys[s] = kEmpty;
+                        vals[s] = CV(0);
+                        dcnt++;
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b < EB; b++)
+                    if (kk[b] != kEmpty) sc[b] = A.sigma[kk[b]];
+#pragma unroll
+                for (int b = 0; b < EB; b++) {
+                    if (kk[b] != kEmpty) {
+                        G gn = Prec<PREC>::gain(kv[b], e_src, ki, a, sc[b], kref<BT>(A, vv));
+                        if (better(gn, kk[b], best, dst, up)) {
+                            best = gn;
+                            dst = kk[b];
+                        }
+                    }
+                }
+            }
+        }
+        for (uint32_t ub = threadIdx.x & ~31u; !DENSE && ub < nd; ub += kClusterThreads * EB) {  // warp-uniform
             const uint32_t u0 = ub + (threadIdx.x & 31u);
             uint32_t kk[EB];
             double kv[EB], sc[EB];
@@ -1093,7 +1129,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
         }
         group_argmax<kClusterThreads, G>(best, dst, up, red_g, red_c);
         if (threadIdx.x == 0) {
-            dcnt += nd;
+            if constexpr (!DENSE) dcnt += nd;
             ucnt = 0;  // every thread of this CTA has read it (barriers in group_argmax)
             rank_ptr<CS>(&best_g[par][0], 0)[rank] = best;
             rank_ptr<CS>(&best_c[par][0], 0)[rank] = dst;
@@ -1322,9 +1358,10 @@ __global__ void heavy_final_kernel(LMArgs A, const uint32_t *hv, uint32_t H, con
     flush_acc(A.acc, A.integral, sin, 0);
 }
 
-template <int CS, int WK, int PREC, int VER, int BT>
+template <int CS, int WK, int PREC, int VER, int BT, bool DENSE>
 size_t cluster_smem() {
-    return (size_t)kSegSlots<WK> * (sizeof(uint32_t) + sizeof(typename ValT<WK>::type) + sizeof(uint16_t));
+    if constexpr (DENSE) return (size_t)kDenseSlots * (sizeof(uint32_t) + sizeof(typename ValT<WK>::type));
+    else return (size_t)kSegSlots<WK> * (sizeof(uint32_t) + sizeof(typename ValT<WK>::type) + sizeof(uint16_t));
 }
 
 template <int CS, int WK, int PREC, int VER, int BT>
@@ -1347,7 +1384,7 @@ cudaLaunchConfig_t cluster_config(size_t smem, unsigned grid, cudaStream_t s, cu
 // run) on the current device.  The first call per device also raises the
 // kernel's shared-memory limit there (a per-device setting); the result is
 // cached per device, under a lock, since serving workers launch concurrently.
-template <int CS, int WK, int PREC, int VER, int BT>
+template <int CS, int WK, int PREC, int VER, int BT, bool DENSE = false>
 int cluster_capacity() {
     static std::mutex mu;
     static std::map<int, int> caps;  // device -> co-resident clusters
@@ -1356,8 +1393,8 @@ int cluster_capacity() {
     std::lock_guard<std::mutex> lk(mu);
     const auto it = caps.find(dev);
     if (it != caps.end()) return it->second;
-    auto kern = lm_cluster_kernel<CS, WK, PREC, VER, BT>;
-    const size_t smem = cluster_smem<CS, WK, PREC, VER, BT>();
+    auto kern = lm_cluster_kernel<CS, WK, PREC, VER, BT, DENSE>;
+    const size_t smem = cluster_smem<CS, WK, PREC, VER, BT, DENSE>();
     MG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (CS > 8) MG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchAttribute attr[1];
@@ -1371,11 +1408,11 @@ int cluster_capacity() {
     return n;
 }
 
-template <int CS, int WK, int PREC, int VER, int BT>
+template <int CS, int WK, int PREC, int VER, int BT, bool DENSE>
 void launch_cluster(const LMArgs &A, const uint32_t *verts, uint32_t count, cudaStream_t s) {
-    auto kern = lm_cluster_kernel<CS, WK, PREC, VER, BT>;
-    const size_t smem = cluster_smem<CS, WK, PREC, VER, BT>();
-    int cap = cluster_capacity<CS, WK, PREC, VER, BT>();
+    auto kern = lm_cluster_kernel<CS, WK, PREC, VER, BT, DENSE>;
+    const size_t smem = cluster_smem<CS, WK, PREC, VER, BT, DENSE>();
+    int cap = cluster_capacity<CS, WK, PREC, VER, BT, DENSE>();
     MG_CHECK(cap > 0, MG_ERR_UNSUPPORTED, "cluster shape cannot be scheduled on this device");
     unsigned clusters = (unsigned)std::min<uint64_t>(count, (uint64_t)cap);
     cudaLaunchAttribute attr[1];
@@ -1663,19 +1700,19 @@ void launch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, c
     const uint32_t *hl = lvl.heavy_list;
     // heavy tiers, largest clusters first
     if (lvl.tier_off[5] > lvl.tier_off[4])
-        launch_cluster<tier_ctas<WK>(4), WK, PREC, VER, BT>(A, hl + lvl.tier_off[4], lvl.tier_off[5] - lvl.tier_off[4],
+        launch_cluster<tier_ctas<WK>(4), WK, PREC, VER, BT, kDenseTier<WK>(4)>(A, hl + lvl.tier_off[4], lvl.tier_off[5] - lvl.tier_off[4],
                                                              sh);
     if (lvl.tier_off[4] > lvl.tier_off[3])
-        launch_cluster<tier_ctas<WK>(3), WK, PREC, VER, BT>(A, hl + lvl.tier_off[3], lvl.tier_off[4] - lvl.tier_off[3],
+        launch_cluster<tier_ctas<WK>(3), WK, PREC, VER, BT, kDenseTier<WK>(3)>(A, hl + lvl.tier_off[3], lvl.tier_off[4] - lvl.tier_off[3],
                                                              sh);
     if (lvl.tier_off[3] > lvl.tier_off[2])
-        launch_cluster<tier_ctas<WK>(2), WK, PREC, VER, BT>(A, hl + lvl.tier_off[2], lvl.tier_off[3] - lvl.tier_off[2],
+        launch_cluster<tier_ctas<WK>(2), WK, PREC, VER, BT, kDenseTier<WK>(2)>(A, hl + lvl.tier_off[2], lvl.tier_off[3] - lvl.tier_off[2],
                                                              sh);
     if (lvl.tier_off[2] > lvl.tier_off[1])
-        launch_cluster<tier_ctas<WK>(1), WK, PREC, VER, BT>(A, hl + lvl.tier_off[1], lvl.tier_off[2] - lvl.tier_off[1],
+        launch_cluster<tier_ctas<WK>(1), WK, PREC, VER, BT, kDenseTier<WK>(1)>(A, hl + lvl.tier_off[1], lvl.tier_off[2] - lvl.tier_off[1],
                                                              sh);
     if (lvl.tier_off[1] > lvl.tier_off[0])
-        launch_cluster<tier_ctas<WK>(0), WK, PREC, VER, BT>(A, hl + lvl.tier_off[0], lvl.tier_off[1] - lvl.tier_off[0],
+        launch_cluster<tier_ctas<WK>(0), WK, PREC, VER, BT, kDenseTier<WK>(0)>(A, hl + lvl.tier_off[0], lvl.tier_off[1] - lvl.tier_off[0],
                                                              sm);
     if (lvl.giants > 0) {
         const uint32_t H = lvl.giants;

@@ -123,10 +123,10 @@ __global__ void level_init_kernel(const uint32_t *off, const void *w, uint32_t n
 }
 
 // Largest cluster size (8 or 16) the device schedules for the heavy tiers.
-// (the largest tier: 16 CTAs for real weights, 12 for integral ones)
+// (the largest tier: 16 CTAs for real weights, 8 dense CTAs for integral ones)
 int probe_max_cluster() {
     return cluster_capacity<tier_ctas<WK_F64>(4), WK_F64, MG_PREC_FP64, 2, 0>() > 0 &&
-                   cluster_capacity<tier_ctas<WK_UNIT>(4), WK_UNIT, MG_PREC_FP64, 2, 0>() > 0
+                   cluster_capacity<tier_ctas<WK_UNIT>(4), WK_UNIT, MG_PREC_FP64, 2, 0, kDenseTier<WK_UNIT>(4)>() > 0
                ? 16
                : 8;
 }
@@ -186,7 +186,8 @@ void move_prepare_level(const GraphView &g, MoveLevel &lvl, MoveWorkspace &ws, c
     if (lvl.heavy == 0) return;
     if (ws.max_cluster == 0) ws.max_cluster = probe_max_cluster();
     // classes 13..17 are the cluster tiers (tier t: tier_ctas(t) CTAs holding
-    // degrees up to tier_ctas(t) * kSegSlots / 2), class 18 the giants; on a
+    // degrees up to 2^(13+t) at load <= 1/2, or <= 2/3 with dense segments),
+    // class 18 the giants; on a
     // device without 12- and 16-CTA clusters class 17 joins the giants, and so
     // do the classes from ws.giant_class on
     int first_giant = std::min(ws.giant_class - kFirstHeavyClass, kTiers - 1);
