@@ -73,17 +73,17 @@ constexpr int kClusterSlots = 16384;
 // 0.69 s.  The dense segments below keep power-of-two clusters and 192 KB.)
 template <int WK>
 constexpr int kSegSlots = kClusterSlots;
-// Dense segments (integral weights, tiers 1-4): 24,576 slots of a 32-bit key
-// and a 32-bit sum (192 KB) and no insertion list -- the evaluation scans the
-// slots -- at table load <= 2/3, so one CTA holds 16,384 distinct communities
-// and the tiers need half the CTAs (every CTA of a cluster reads the whole
-// row with the own fill).  Tier 0 (degrees <= 8,192) keeps the list, which
-// spares its short rows a scan of the whole segment.
+// Dense segments (integral weights): 24,576 slots of a 32-bit key and a
+// 32-bit sum (192 KB) per 1,024-thread CTA and no insertion list -- the
+// evaluation scans the slots -- at table load <= 2/3, so one CTA holds 16,384
+// distinct communities and tiers 1-4 need half the CTAs of listed segments
+// (every CTA of a cluster reads the whole row with the own fill).  Tier 0
+// (degrees <= 8,192) runs 512-thread CTAs with half a segment.
 constexpr int kDenseSlots = 24576;
 constexpr int kDenseCapacity = kDenseSlots / 3 * 2;
 template <int WK>
-constexpr bool kDenseTier(int t) {
-    return kIntg<WK> && t >= 1;
+constexpr bool kDenseTier(int /*t*/) {
+    return kIntg<WK>;
 }
 // CTAs of the cluster serving heavy tier t (degree class 13 + t, degrees up
 // to 2^(13+t)): 1, 2, 4, 8, 16 at table load <= 1/2 with the listed segments,

@@ -905,6 +905,13 @@ __global__ void __launch_bounds__(kWarpThreads) lm_warp_kernel(LMArgs A, uint32_
 // ============================================================================
 namespace cg = cooperative_groups;
 constexpr int kClusterThreads = 1024;  // one CTA per SM with a 16K-slot segment
+// CTA size of heavy tier t: tier 0 of an integral graph (degrees <= 8,192)
+// runs 512-thread CTAs with half a dense segment, two per SM, so that one
+// vertex's barriers and argmax overlap another's edge pass
+template <int WK>
+constexpr int tier_threads(int t) {
+    return kDenseTier<WK>(t) && t == 0 ? kClusterThreads / 2 : kClusterThreads;
+}
 
 template <int CS>
 __device__ __forceinline__ void cluster_barrier() {
@@ -918,13 +925,13 @@ __device__ __forceinline__ T *rank_ptr(T *p, unsigned r) {
     else return cg::this_cluster().map_shared_rank(p, r);
 }
 
-template <int CS, int WK, int PREC, int VER, int BT, bool DENSE = false>
-__global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A, const uint32_t *verts,
+template <int CS, int WK, int PREC, int VER, int BT, bool DENSE = false, int NT = kClusterThreads>
+__global__ void __launch_bounds__(NT, kClusterThreads / NT) lm_cluster_kernel(LMArgs A, const uint32_t *verts,
                                                                         uint32_t count) {
     using G = typename Prec<PREC>::G;
     const int up = load_up<BT>(A);
     static_assert(!DENSE || kIntg<WK>, "dense segments hold 32-bit sums");
-    constexpr int S = DENSE ? kDenseSlots : kSegSlots<WK>;
+    constexpr int S = DENSE ? kDenseSlots / (kClusterThreads / NT) : kSegSlots<WK>;
     constexpr int BATCH = 4;
     constexpr int EB = 4;  // slots per thread per evaluation batch
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -943,7 +950,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
     __shared__ uint32_t red_c[32];
     unsigned rank = 0;
     if constexpr (CS > 1) rank = cg::this_cluster().block_rank();
-    for (int s = threadIdx.x; s < S; s += kClusterThreads) {
+    for (int s = threadIdx.x; s < S; s += NT) {
         keys[s] = kEmpty;
         vals[s] = CV(0);
     }
@@ -974,8 +981,8 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
         //    the owner CTA, through distributed shared memory when it is
         //    another.
         const bool own = CS > 1 && !A.split;
-        const uint32_t t0 = own ? threadIdx.x : rank * kClusterThreads + threadIdx.x;
-        const uint32_t step = own ? kClusterThreads : CS * kClusterThreads;
+        const uint32_t t0 = own ? threadIdx.x : rank * NT + threadIdx.x;
+        const uint32_t step = own ? NT : CS * NT;
         // add `val` to community `key`'s slot in the segment of its owner CTA
         // (this CTA's own shared memory, or another's through DSMEM)
         auto ins = [&](uint32_t key, CV val) {
@@ -1060,15 +1067,15 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
         const uint32_t nd = ucnt;
         if constexpr (DENSE) {
             // every slot of the segment, EB per thread per step (S is a
-            // multiple of kClusterThreads * EB); the non-empty ones are this
+            // multiple of NT * EB); the non-empty ones are this
             // CTA's candidates, reset as they are read
-            static_assert(S % (kClusterThreads * EB) == 0, "whole evaluation steps");
-            for (uint32_t sb = threadIdx.x; sb < (uint32_t)S; sb += kClusterThreads * EB) {
+            static_assert(S % (NT * EB) == 0, "whole evaluation steps");
+            for (uint32_t sb = threadIdx.x; sb < (uint32_t)S; sb += NT * EB) {
                 uint32_t kk[EB];
                 double kv[EB], sc[EB];
 #pragma unroll
                 for (int b = 0; b < EB; b++) {
-                    const uint32_t s = sb + b * kClusterThreads;
+                    const uint32_t s = sb + b * NT;
                     kk[b] = keys[s];
                     if (kk[b] != kEmpty) {
                         kv[b] = v2d(vals[s]);
@@ -1092,7 +1099,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
                 }
             }
         }
-        for (uint32_t ub = threadIdx.x & ~31u; !DENSE && ub < nd; ub += kClusterThreads * EB) {  // warp-uniform
+        for (uint32_t ub = threadIdx.x & ~31u; !DENSE && ub < nd; ub += NT * EB) {  // warp-uniform
             const uint32_t u0 = ub + (threadIdx.x & 31u);
             uint32_t kk[EB];
             double kv[EB], sc[EB];
@@ -1100,8 +1107,8 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
 #pragma unroll
             for (int b = 0; b < EB; b++) {
                 kk[b] = kEmpty;
-                if (ub + b * kClusterThreads >= nd) break;
-                const uint32_t u = u0 + b * kClusterThreads;
+                if (ub + b * NT >= nd) break;
+                const uint32_t u = u0 + b * NT;
                 if (u < nd) {
                     const uint32_t s = used[u];
                     kk[b] = keys[s];
@@ -1112,12 +1119,12 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
             }
 #pragma unroll
             for (int b = 0; b < EB; b++) {
-                if (ub + b * kClusterThreads >= nd) break;
+                if (ub + b * NT >= nd) break;
                 if (kk[b] != kEmpty) sc[b] = A.sigma[kk[b]];
             }
 #pragma unroll
             for (int b = 0; b < EB; b++) {
-                if (ub + b * kClusterThreads >= nd) break;
+                if (ub + b * NT >= nd) break;
                 if (kk[b] != kEmpty) {
                     G gn = Prec<PREC>::gain(kv[b], e_src, ki, a, sc[b], kref<BT>(A, vv));
                     if (better(gn, kk[b], best, dst, up)) {
@@ -1127,7 +1134,7 @@ __global__ void __launch_bounds__(kClusterThreads, 1) lm_cluster_kernel(LMArgs A
                 }
             }
         }
-        group_argmax<kClusterThreads, G>(best, dst, up, red_g, red_c);
+        group_argmax<NT, G>(best, dst, up, red_g, red_c);
         if (threadIdx.x == 0) {
             if constexpr (!DENSE) dcnt += nd;
             ucnt = 0;  // every thread of this CTA has read it (barriers in group_argmax)
@@ -1358,17 +1365,18 @@ __global__ void heavy_final_kernel(LMArgs A, const uint32_t *hv, uint32_t H, con
     flush_acc(A.acc, A.integral, sin, 0);
 }
 
-template <int CS, int WK, int PREC, int VER, int BT, bool DENSE>
+template <int CS, int WK, int PREC, int VER, int BT, bool DENSE, int NT = kClusterThreads>
 size_t cluster_smem() {
-    if constexpr (DENSE) return (size_t)kDenseSlots * (sizeof(uint32_t) + sizeof(typename ValT<WK>::type));
+    if constexpr (DENSE)
+        return (size_t)(kDenseSlots / (kClusterThreads / NT)) * (sizeof(uint32_t) + sizeof(typename ValT<WK>::type));
     else return (size_t)kSegSlots<WK> * (sizeof(uint32_t) + sizeof(typename ValT<WK>::type) + sizeof(uint16_t));
 }
 
-template <int CS, int WK, int PREC, int VER, int BT>
+template <int CS, int WK, int PREC, int VER, int BT, int NT = kClusterThreads>
 cudaLaunchConfig_t cluster_config(size_t smem, unsigned grid, cudaStream_t s, cudaLaunchAttribute *attr) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid, 1, 1);
-    cfg.blockDim = dim3(kClusterThreads, 1, 1);
+    cfg.blockDim = dim3(NT, 1, 1);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1384,7 +1392,7 @@ cudaLaunchConfig_t cluster_config(size_t smem, unsigned grid, cudaStream_t s, cu
 // run) on the current device.  The first call per device also raises the
 // kernel's shared-memory limit there (a per-device setting); the result is
 // cached per device, under a lock, since serving workers launch concurrently.
-template <int CS, int WK, int PREC, int VER, int BT, bool DENSE = false>
+template <int CS, int WK, int PREC, int VER, int BT, bool DENSE = false, int NT = kClusterThreads>
 int cluster_capacity() {
     static std::mutex mu;
     static std::map<int, int> caps;  // device -> co-resident clusters
@@ -1393,12 +1401,12 @@ int cluster_capacity() {
     std::lock_guard<std::mutex> lk(mu);
     const auto it = caps.find(dev);
     if (it != caps.end()) return it->second;
-    auto kern = lm_cluster_kernel<CS, WK, PREC, VER, BT, DENSE>;
-    const size_t smem = cluster_smem<CS, WK, PREC, VER, BT, DENSE>();
+    auto kern = lm_cluster_kernel<CS, WK, PREC, VER, BT, DENSE, NT>;
+    const size_t smem = cluster_smem<CS, WK, PREC, VER, BT, DENSE, NT>();
     MG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (CS > 8) MG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = cluster_config<CS, WK, PREC, VER, BT>(smem, CS * 148, nullptr, attr);
+    cudaLaunchConfig_t cfg = cluster_config<CS, WK, PREC, VER, BT, NT>(smem, CS * 148, nullptr, attr);
     int n = 0;
     if (cudaOccupancyMaxActiveClusters(&n, (void *)kern, &cfg) != cudaSuccess) {
         cudaGetLastError();
@@ -1408,15 +1416,15 @@ int cluster_capacity() {
     return n;
 }
 
-template <int CS, int WK, int PREC, int VER, int BT, bool DENSE>
+template <int CS, int WK, int PREC, int VER, int BT, bool DENSE, int NT = kClusterThreads>
 void launch_cluster(const LMArgs &A, const uint32_t *verts, uint32_t count, cudaStream_t s) {
-    auto kern = lm_cluster_kernel<CS, WK, PREC, VER, BT, DENSE>;
-    const size_t smem = cluster_smem<CS, WK, PREC, VER, BT, DENSE>();
-    int cap = cluster_capacity<CS, WK, PREC, VER, BT, DENSE>();
+    auto kern = lm_cluster_kernel<CS, WK, PREC, VER, BT, DENSE, NT>;
+    const size_t smem = cluster_smem<CS, WK, PREC, VER, BT, DENSE, NT>();
+    int cap = cluster_capacity<CS, WK, PREC, VER, BT, DENSE, NT>();
     MG_CHECK(cap > 0, MG_ERR_UNSUPPORTED, "cluster shape cannot be scheduled on this device");
     unsigned clusters = (unsigned)std::min<uint64_t>(count, (uint64_t)cap);
     cudaLaunchAttribute attr[1];
-    cudaLaunchConfig_t cfg = cluster_config<CS, WK, PREC, VER, BT>(smem, clusters * CS, s, attr);
+    cudaLaunchConfig_t cfg = cluster_config<CS, WK, PREC, VER, BT, NT>(smem, clusters * CS, s, attr);
     MG_CUDA(cudaLaunchKernelEx(&cfg, kern, A, verts, count));
     MG_LAUNCH_CHECK();
 }
@@ -1712,7 +1720,7 @@ void launch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, c
         launch_cluster<tier_ctas<WK>(1), WK, PREC, VER, BT, kDenseTier<WK>(1)>(A, hl + lvl.tier_off[1], lvl.tier_off[2] - lvl.tier_off[1],
                                                              sh);
     if (lvl.tier_off[1] > lvl.tier_off[0])
-        launch_cluster<tier_ctas<WK>(0), WK, PREC, VER, BT, kDenseTier<WK>(0)>(A, hl + lvl.tier_off[0], lvl.tier_off[1] - lvl.tier_off[0],
+        launch_cluster<tier_ctas<WK>(0), WK, PREC, VER, BT, kDenseTier<WK>(0), tier_threads<WK>(0)>(A, hl + lvl.tier_off[0], lvl.tier_off[1] - lvl.tier_off[0],
                                                              sm);
     if (lvl.giants > 0) {
         const uint32_t H = lvl.giants;
