@@ -310,7 +310,7 @@ typedef struct {
     int cluster_fill;    /* MG_FILL_* */
     int giant_class;     /* degree classes >= this (13..18) take the global-table path; 0 = default (18) */
     int coarsen_combine; /* MG_COMBINE_* */
-    int light_streams;   /* streams the light degree classes are spread over, 1..7 (0 = default 2) */
+    int light_streams;   /* streams the light degree classes are spread over, 1..7 (0 = default 1) */
     int table_first_sweep; /* 1: a level's first sweep uses the table kernels too (default 0: every
                               community is one vertex there, so it runs table-free kernels) */
 } mg_sweep_opts;

@@ -183,10 +183,11 @@ struct MoveWorkspace {
     TuneTable tune;
     PrimWorkspace prim;
     // stream 0: heavy tiers; streams 1..light_streams: the light classes and
-    // the 1-CTA cluster tier, so that one class's tail overlaps the others
-    // (two by default: more streams measured slower on R-MAT-24)
+    // the class-13 tier, so that one class's tail overlaps the others (one by
+    // default: with the dense cluster tiers, R-MAT-24 ran 0.4593 s on one,
+    // 0.4635 s on two, 0.4605 s on three, 0.4635 s on four)
     static constexpr int kStreams = 8;
-    static constexpr int kDefaultLightStreams = 2;
+    static constexpr int kDefaultLightStreams = 1;
     cudaStream_t streams[kStreams] = {};
     cudaEvent_t ev_fork = nullptr, ev_join[kStreams] = {};
     int light_streams = kDefaultLightStreams;

@@ -418,3 +418,15 @@ def test_first_sweep_kernels_equal_table_kernels(O, ctx):
             assert abs(dg.louvain()["modularity"] - ref["modularity"]) <= 1e-3
     finally:
         ctx.sweep_options()
+
+
+@pytest.mark.parametrize("streams", [1, 3, 7])
+def test_light_streams_do_not_change_results(O, ctx, streams):
+    """The light classes on 1, 3 or 7 streams beside the heavy stream: the
+    oracle's run bit for bit."""
+    ctx.sweep_options(light_streams=streams)
+    try:
+        g = O.gen_rmat(14, seed=2)
+        _compare_runs(_up(ctx, g).louvain(), O.louvain(g))
+    finally:
+        ctx.sweep_options()
