@@ -7,11 +7,16 @@ oracle/build_ref.sh with the single-PE shim) on small seeded graphs:
   * one local-move sweep, versions 1 and 2 (src/louvain/louvain.cu:1032, louvain_gl.cu:1018)
   * coarsen_graph_mg::coarsen_graph        (src/coarsen_graph/coarsen_graph_mg.cu:2054)
   * louvain*::run printed tables           (src/louvain/louvain*.cu run())
+and, with --traces, the printed tables alone (versions 0, 1 and 2) on two
+larger seeded graphs -- the 65,536-vertex SBM of the plain-Louvain workload and
+R-MAT scale 16 -- into traces.json (the graphs are regenerated from their
+seeds by the oracle's and the engine's generators, so only the tables and a
+checksum of each graph are stored).
 The inputs (graphs, assignments, sigma, k) come from the CPU oracle's seeded
 generators and are stored with the outputs, so the fixtures are
 self-contained.  Needs a CUDA GPU for everything but the loader.
 
-Usage: python tests/golden/make_golden.py [--out DIR]
+Usage: python tests/golden/make_golden.py [--out DIR] [--traces]
 """
 from __future__ import annotations
 
@@ -108,6 +113,43 @@ def cases():
     return out
 
 
+# larger graphs whose reference traces are kept (generator, arguments)
+TRACE_CASES = (
+    ("sbm64k", "sbm", dict(n=65536, blocks=64, mean_degree=16.0, intra_frac=0.8, seed=1)),
+    ("rmat16", "rmat", dict(scale=16, seed=2)),
+)
+
+
+def trace_graph(kind, kw):
+    return O.gen_sbm(**kw) if kind == "sbm" else O.gen_rmat(**kw)
+
+
+def graph_checksum(g):
+    """Order-sensitive digest of a CSR (offsets and column ids), the same on every host."""
+    import hashlib
+    h = hashlib.sha256()
+    h.update(np.asarray(g.offsets, np.uint64).tobytes())
+    h.update(np.asarray(g.cols, np.uint32).tobytes())
+    return h.hexdigest()
+
+
+def make_traces(out):
+    tmp = tempfile.mkdtemp()
+    res = {}
+    for name, kind, kw in TRACE_CASES:
+        g = trace_graph(kind, kw)
+        mtx = os.path.join(tmp, name + ".mtx")
+        write_mtx(mtx, g, False)
+        entry = {"generator": kind, "args": kw, "n": int(g.n), "nnz": int(len(g.cols)),
+                 "sha256": graph_checksum(g), "trace": {}}
+        for version in (0, 1, 2):
+            entry["trace"][str(version)] = parse_table(run("louvain", mtx, version))
+        res[name] = entry
+        print("trace", name, g.n, len(g.cols), flush=True)
+    with open(os.path.join(out, "traces.json"), "w") as f:
+        json.dump(res, f, indent=1)
+
+
 def states(g, k, mass):
     res = [("start", np.arange(g.n, dtype=np.uint32), k.copy())]
     C = np.arange(g.n, dtype=np.uint32)
@@ -124,8 +166,12 @@ def states(g, k, mass):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
+    ap.add_argument("--traces", action="store_true", help="only the larger graphs' printed tables")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
+    if a.traces:
+        make_traces(a.out)
+        return
     tmp = tempfile.mkdtemp()
     for name, g, weighted in cases():
         mtx = os.path.join(tmp, name + ".mtx")

@@ -9,6 +9,7 @@ Real-weight cases (chunglu4k) use tolerances: the reference sums with FP64
 atomics in an unspecified order.
 """
 import glob
+import hashlib
 import json
 import os
 
@@ -139,3 +140,58 @@ def test_engine_against_reference(O, ctx, name):
 
     _check_coarsen(co, z, exact)
     _check_trace(lambda v: dg.louvain(version=v)["trace"], meta, exact)
+
+
+# ---- larger graphs: the reference's printed tables only (tests/golden/traces.json) ----------
+
+TRACES = os.path.join(GOLDEN, "traces.json")
+TRACE_NAMES = sorted(json.load(open(TRACES))) if os.path.exists(TRACES) else []
+
+
+def _trace_case(name):
+    return json.load(open(TRACES))[name]
+
+
+def _trace_graph(O, meta):
+    kw = dict(meta["args"])
+    return O.gen_sbm(**kw) if meta["generator"] == "sbm" else O.gen_rmat(**kw)
+
+
+def _digest(off, cols):
+    h = hashlib.sha256()
+    h.update(np.asarray(off, np.uint64).tobytes())
+    h.update(np.asarray(cols, np.uint32).tobytes())
+    return h.hexdigest()
+
+
+def test_trace_fixtures_present():
+    if not TRACE_NAMES:
+        pytest.skip("reference traces not generated yet (make_golden.py --traces on a GPU host)")
+    assert {"sbm64k", "rmat16"} <= set(TRACE_NAMES)
+
+
+@pytest.mark.parametrize("name", TRACE_NAMES)
+def test_oracle_trace_against_reference(O, name):
+    """The oracle's Louvain on the regenerated graph prints the reference's table:
+    same phases and loops, Q to the printed 6 decimals (versions 0/1/2)."""
+    meta = _trace_case(name)
+    g = _trace_graph(O, meta)
+    assert (g.n, len(g.cols)) == (meta["n"], meta["nnz"])
+    assert _digest(g.offsets, g.cols) == meta["sha256"]
+    _check_trace(lambda v: O.louvain(g, version=2 if v == 0 else v)["trace"], meta, True)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", TRACE_NAMES)
+def test_engine_trace_against_reference(ctx, name):
+    """The engine's generator gives the reference's input graph (same digest) and
+    its Louvain run prints the reference's table (versions 0/1/2)."""
+    meta = _trace_case(name)
+    kw = dict(meta["args"])
+    if meta["generator"] == "sbm":
+        dg = ctx.generate_sbm(kw["n"], kw["blocks"], kw["mean_degree"], kw["intra_frac"], kw["seed"])
+    else:
+        dg = ctx.generate_rmat(kw["scale"], seed=kw["seed"])
+    off, cols, _ = dg.csr()
+    assert _digest(off, cols) == meta["sha256"]
+    _check_trace(lambda v: dg.louvain(version=v)["trace"], meta, True)
