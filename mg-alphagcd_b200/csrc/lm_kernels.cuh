@@ -1451,6 +1451,15 @@ inline void raise_smem_limit(const void *kern, size_t smem) {
     done.insert({kern, dev});
 }
 
+// Shared-memory carveout (percent of the SM's 228 KB) that holds `blocks`
+// resident blocks of `smem` dynamic bytes each (plus static shared memory and
+// the per-block reserve): the rest of the SM's 256 KB stays L1, where the
+// community and sigma gathers of the table kernels hit.
+inline unsigned carveout_pct(size_t smem, int blocks) {
+    const size_t need = (size_t)blocks * (smem + 2048);
+    return (unsigned)std::min<size_t>(100, (need * 100 + 233471) / 233472 + 1);
+}
+
 // One light class (degrees <= 2^cls) with the given shape.
 template <int WK, int PREC, int VER, int BT>
 void launch_light(int shape, int cls, const LMArgs &A, uint32_t off, uint32_t size, cudaStream_t s) {
@@ -1470,7 +1479,23 @@ void launch_light(int shape, int cls, const LMArgs &A, uint32_t off, uint32_t si
         while ((1u << max_sl) < 2 * shape_capacity(shape)) max_sl++;
         raise_smem_limit((const void *)kern, hash_smem<WK>(gpb, max_sl));
         const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(size, gpb), 148ull * 64);
-        kern<<<grid, block, smem, s>>>(A, off, size, sl);
+        if constexpr (BT == 0) {
+            // single-graph sweeps: the smallest carveout that keeps the
+            // launch's occupancy (1024 / block resident blocks)
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(grid);
+            cfg.blockDim = dim3(block);
+            cfg.dynamicSmemBytes = smem;
+            cfg.stream = s;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributePreferredSharedMemoryCarveout;
+            at[0].val.sharedMemCarveout = carveout_pct(smem, 1024 / block);
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            MG_CUDA(cudaLaunchKernelEx(&cfg, kern, A, off, size, sl));
+        } else {
+            kern<<<grid, block, smem, s>>>(A, off, size, sl);
+        }
         MG_LAUNCH_CHECK();
     };
     auto warpk = [&](auto kern) {
