@@ -9,6 +9,7 @@
 #include <map>
 #include <mutex>
 #include <set>
+#include <tuple>
 #include <utility>
 #include <vector>
 
@@ -1452,12 +1453,56 @@ inline void raise_smem_limit(const void *kern, size_t smem) {
 }
 
 // Shared-memory carveout (percent of the SM's 228 KB) that holds `blocks`
-// resident blocks of `smem` dynamic bytes each (plus static shared memory and
-// the per-block reserve): the rest of the SM's 256 KB stays L1, where the
-// community and sigma gathers of the table kernels hit.
-inline unsigned carveout_pct(size_t smem, int blocks) {
-    const size_t need = (size_t)blocks * (smem + 2048);
+// resident blocks of `smem` dynamic and `stat` static bytes each (plus the
+// per-block reserve): the rest of the SM's 256 KB stays L1, where the
+// community and sigma gathers of the sweep kernels hit.
+inline unsigned carveout_pct(size_t smem, size_t stat, int blocks) {
+    const size_t need = (size_t)blocks * (smem + stat + 1024);
     return (unsigned)std::min<size_t>(100, (need * 100 + 233471) / 233472 + 1);
+}
+
+// The carveout of a kernel launched with `block` threads and `smem` dynamic
+// bytes: the smallest that keeps its full occupancy (occupancy calculator,
+// which assumes the largest carveout), cached per device under a lock since
+// serving workers launch concurrently.
+inline unsigned launch_carveout(const void *kern, unsigned block, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::tuple<const void *, unsigned, size_t, int>, unsigned> cache;
+    int dev = 0;
+    MG_CUDA(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(kern, block, smem, dev);
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int blocks = 0;
+    MG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, (int)block, smem));
+    cudaFuncAttributes fa;
+    MG_CUDA(cudaFuncGetAttributes(&fa, kern));
+    const unsigned pct = blocks > 0 ? carveout_pct(smem, fa.sharedSizeBytes, blocks) : 100u;
+    cache.emplace(key, pct);
+    return pct;
+}
+
+// Launch of a single-graph sweep kernel with its carveout hint (batched sweeps
+// launch plainly: they are captured into CUDA graphs).
+template <int BT, class... P, class... Args>
+void launch_l1(void (*kern)(P...), unsigned grid, unsigned block, size_t smem, cudaStream_t s, Args... args) {
+    if constexpr (BT == 0) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(grid);
+        cfg.blockDim = dim3(block);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributePreferredSharedMemoryCarveout;
+        at[0].val.sharedMemCarveout = launch_carveout((const void *)kern, block, smem);
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        MG_CUDA(cudaLaunchKernelEx(&cfg, kern, args...));
+    } else {
+        kern<<<grid, block, smem, s>>>(args...);
+    }
+    MG_LAUNCH_CHECK();
 }
 
 // One light class (degrees <= 2^cls) with the given shape.
@@ -1467,8 +1512,7 @@ void launch_light(int shape, int cls, const LMArgs &A, uint32_t off, uint32_t si
     auto tile = [&](auto kern, int T) {
         const uint64_t per_block = 256 / T;
         const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(size, per_block), 148ull * 32);
-        kern<<<grid, 256, 0, s>>>(A, off, size);
-        MG_LAUNCH_CHECK();
+        launch_l1<BT>(kern, grid, 256, 0, s, A, off, size);
     };
     auto hash = [&](auto kern, int gt, int block) {
         const int gpb = block / gt;
@@ -1479,24 +1523,7 @@ void launch_light(int shape, int cls, const LMArgs &A, uint32_t off, uint32_t si
         while ((1u << max_sl) < 2 * shape_capacity(shape)) max_sl++;
         raise_smem_limit((const void *)kern, hash_smem<WK>(gpb, max_sl));
         const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(size, gpb), 148ull * 64);
-        if constexpr (BT == 0) {
-            // single-graph sweeps: the smallest carveout that keeps the
-            // launch's occupancy (1024 / block resident blocks)
-            cudaLaunchConfig_t cfg = {};
-            cfg.gridDim = dim3(grid);
-            cfg.blockDim = dim3(block);
-            cfg.dynamicSmemBytes = smem;
-            cfg.stream = s;
-            cudaLaunchAttribute at[1];
-            at[0].id = cudaLaunchAttributePreferredSharedMemoryCarveout;
-            at[0].val.sharedMemCarveout = carveout_pct(smem, 1024 / block);
-            cfg.attrs = at;
-            cfg.numAttrs = 1;
-            MG_CUDA(cudaLaunchKernelEx(&cfg, kern, A, off, size, sl));
-        } else {
-            kern<<<grid, block, smem, s>>>(A, off, size, sl);
-        }
-        MG_LAUNCH_CHECK();
+        launch_l1<BT>(kern, grid, block, smem, s, A, off, size, sl);
     };
     auto warpk = [&](auto kern) {
         const int logd = std::max(5, cls);
@@ -1504,8 +1531,7 @@ void launch_light(int shape, int cls, const LMArgs &A, uint32_t off, uint32_t si
         raise_smem_limit((const void *)kern, (kWarpThreads / 32) * warp_slice_bytes<WK>(kWarpMaxLogD));
         const uint32_t K = (1u << logd) >= (uint32_t)kWarpF ? 1u : (uint32_t)kWarpF >> logd;
         const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(size, (kWarpThreads / 32) * K), 148ull * 8);
-        kern<<<grid, kWarpThreads, smem, s>>>(A, off, size, logd);
-        MG_LAUNCH_CHECK();
+        launch_l1<BT>(kern, grid, kWarpThreads, smem, s, A, off, size, logd);
     };
     switch (shape) {
         case SH_T2: tile(lm_tile_kernel<2, WK, PREC, VER, BT>, 2); break;
@@ -1690,13 +1716,11 @@ void launch_first(int cls, const LMArgs &A, uint32_t off, uint32_t size, cudaStr
     if (size == 0) return;
     auto lanes = [&](auto kern, int T) {
         const unsigned grid = (unsigned)std::min<uint64_t>(ceil_div(size, 256 / T), 148ull * 32);
-        kern<<<grid, 256, 0, s>>>(A, off, size);
-        MG_LAUNCH_CHECK();
+        launch_l1<0>(kern, grid, 256, 0, s, A, off, size);
     };
     auto block = [&](auto kern, int bs) {
         const unsigned grid = (unsigned)std::min<uint64_t>(size, 148ull * (2048 / bs) * 4);
-        kern<<<grid, bs, 0, s>>>(A, off, size);
-        MG_LAUNCH_CHECK();
+        launch_l1<0>(kern, grid, (unsigned)bs, 0, s, A, off, size);
     };
     if (cls <= 1) lanes(lm_first_kernel<2, WK, PREC, VER>, 2);
     else if (cls == 2) lanes(lm_first_kernel<4, WK, PREC, VER>, 4);
@@ -1750,14 +1774,12 @@ void launch_sweep(const GraphView &g, const MoveLevel &lvl, MoveWorkspace &ws, c
     if (lvl.giants > 0) {
         const uint32_t H = lvl.giants;
         const uint32_t *hv = hl + lvl.tier_off[kTiers - 1];
-        heavy_insert_kernel<WK, VER, BT><<<lvl.ins_items, kHeavyThreads, 0, sh>>>(
-            A, hv, H, ws.h_ins.get(), ws.h_toff.get(), ws.h_tsize.get(), ws.h_keys.get(), ws.h_vals.get(),
-            ws.h_acc.get());
-        MG_LAUNCH_CHECK();
-        heavy_eval_kernel<PREC, BT><<<lvl.eval_items, kHeavyThreads, 0, sh>>>(
-            A, hv, H, ws.h_eval.get(), ws.h_toff.get(), ws.h_tsize.get(), ws.h_keys.get(), ws.h_vals.get(),
-            ws.h_acc.get(), ws.h_best.get());
-        MG_LAUNCH_CHECK();
+        launch_l1<BT>(heavy_insert_kernel<WK, VER, BT>, lvl.ins_items, kHeavyThreads, 0, sh, A, hv, H,
+                      ws.h_ins.get(), ws.h_toff.get(), ws.h_tsize.get(), ws.h_keys.get(), ws.h_vals.get(),
+                      ws.h_acc.get());
+        launch_l1<BT>(heavy_eval_kernel<PREC, BT>, lvl.eval_items, kHeavyThreads, 0, sh, A, hv, H,
+                      ws.h_eval.get(), ws.h_toff.get(), ws.h_tsize.get(), ws.h_keys.get(), ws.h_vals.get(),
+                      ws.h_acc.get(), ws.h_best.get());
         heavy_final_kernel<PREC, VER, BT><<<(unsigned)ceil_div(H, 256), 256, 0, sh>>>(A, hv, H, ws.h_eval.get(),
                                                                                   ws.h_acc.get(), ws.h_best.get());
         MG_LAUNCH_CHECK();
