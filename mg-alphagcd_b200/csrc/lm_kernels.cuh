@@ -1454,8 +1454,10 @@ inline void raise_smem_limit(const void *kern, size_t smem) {
 
 // Shared-memory carveout (percent of the SM's 228 KB) that holds `blocks`
 // resident blocks of `smem` dynamic and `stat` static bytes each (plus the
-// per-block reserve): the rest of the SM's 256 KB stays L1, where the
-// community and sigma gathers of the sweep kernels hit.
+// per-block reserve); the rest of the SM's 256 KB stays L1, which the sweep
+// kernels' community and sigma gathers go through.  The hint pays when the
+// sweep's two streams run kernels concurrently (a kernel running alone gets
+// the same configuration with or without it).
 inline unsigned carveout_pct(size_t smem, size_t stat, int blocks) {
     const size_t need = (size_t)blocks * (smem + stat + 1024);
     return (unsigned)std::min<size_t>(100, (need * 100 + 233471) / 233472 + 1);
